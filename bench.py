@@ -1,0 +1,326 @@
+#!/usr/bin/env python
+"""Benchmark: time-to-converged-labels of EGG-SynC on one B200.
+
+Workload: 1,000,000 x 3 points, 50 Gaussian clusters (centres U[0.1,0.9]^3,
+per-cluster std U[0.005,0.03]), 10% uniform noise, min-max normalised,
+eps = 0.015 (eggsync.data.c5, seed 0).  One step = one full EGG-SynC run
+from positions to converged labels.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+* value: seconds per run with the input already in HBM and the labels left
+  in HBM (device buffers through the C ABI), CUDA events on the calling
+  stream, L2 flushed (256 MiB write) before every timed step.
+* e2e: the same through the public API with pinned host buffers: the
+  host-to-device copy of the points and the device-to-host copy of the labels
+  are inside every timed step.
+* roofline: the update kernel (the dominant kernel), timed with CUDA events
+  on its launching stream in a profiled run.
+* cpu_baseline: the reference's own CPU SynC (src/algorithms/SynC.cpp, built
+  from its sources into oracle/_ref) on a bounded sample of the same workload.
+
+With --gpus N (under torchrun) every rank runs its own replica (the loop does
+not shard); value is the max over ranks.  --impl reference times the
+reference's CPU SynC on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from datetime import timedelta
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "egg-sync_b200"))
+
+METRIC = "time-to-converged-labels (s) at 1M x 3D"
+WORKLOAD = "egg-sync plain loop, 1M x 3D, 50 Gaussian clusters + 10% noise, eps 0.015 (c5 shape, seed 0)"
+L2_FLUSH_BYTES = 256 << 20
+# Iterations the reference EGG semantics take on this workload (measured by
+# the plain GPU path; used only to extrapolate the CPU baseline).
+C5_ITERATIONS = None
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--cpu-sample", type=int, default=0, help="points in the CPU-baseline sample (0 = auto)")
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() and args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=120))
+        pg = dist
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return rank, local, world, pg
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = Path("/tmp/egg_bench_clocks_%d.csv" % os.getpid())
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not self.path.exists():
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        try:
+            self.path.unlink()
+        except Exception:
+            pass
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def update_bytes_per_launch(n, d, cells):
+    """Algorithmic bytes of one update launch: read each point's position and
+    its (sin, 1-cos) offsets once, read each cell's record (start, dims, two
+    sums) once, write each point's new position."""
+    return n * (4 * d + 8 * d + 4 * d) + cells * (4 + 4 * d + 8 * d)
+
+
+def cpu_baseline(X, eps, iterations, sample, seed=0):
+    """Reference CPU SynC (SynC.cpp:16-56, OpenMP) on `sample` points of one
+    iteration against all n points; extrapolated to n points x iterations."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    from oracle import RefSync
+
+    R = RefSync()
+    n = len(X)
+    idx = np.random.default_rng(seed).choice(n, sample, replace=False).astype(np.int32)
+    t0 = time.perf_counter()
+    R.step_sample(X, eps, idx)
+    dt = time.perf_counter() - t0
+    per_point = dt / sample
+    return {
+        "value": per_point * n * iterations,
+        "unit": "s",
+        "cores": R.threads(),
+        "kind": "reference",
+        "sample": "reference SynC parallel (OpenMP) one iteration for %d of %d points against all %d, %.2f s; "
+                  "extrapolated x%d points x %d iterations (EGG iteration count)" % (sample, n, n, dt, n, iterations),
+    }
+
+
+def run_ours(args, rank, local, world, pg):
+    import torch
+
+    from eggsync import data, egg_sync
+
+    dev = torch.device("cuda", local)
+    c = data.c5(args.seed, n=args.n)
+    X, eps = c["X"], c["eps"]
+    n, d = X.shape
+    Xd = torch.from_numpy(X).to(dev)
+    lab_d = torch.empty(n, dtype=torch.int32, device=dev)
+    Xh = torch.from_numpy(X).pin_memory()
+    lab_h = torch.empty(n, dtype=torch.int32).pin_memory()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    for _ in range(max(args.warmup, 0)):
+        _, info = egg_sync(Xd, eps, labels_out=lab_d)
+    egg_sync(Xh.numpy(), eps, labels_out=lab_h.numpy())
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    def timed(fn):
+        times = []
+        barrier()
+        torch.cuda.synchronize(dev)
+        for _ in range(args.steps):
+            flush.zero_()
+            s = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            out = fn()
+            e.record(stream)
+            e.synchronize()
+            times.append(s.elapsed_time(e))
+        torch.cuda.synchronize(dev)
+        barrier()
+        return times, out
+
+    with Clocks(local) as clk:
+        dev_times, (lab, info) = timed(lambda: egg_sync(Xd, eps, labels_out=lab_d))
+    clocks = clk.summary()
+    e2e_times, (lab2, info2) = timed(lambda: egg_sync(Xh.numpy(), eps, labels_out=lab_h.numpy()))
+    assert np.array_equal(lab_d.cpu().numpy(), lab_h.numpy()), "device and host-buffer runs disagree"
+
+    # profiled run: every kernel group bracketed by CUDA events on its stream
+    _, pinfo = egg_sync(Xd, eps, labels_out=lab_d, profile=True)
+
+    ms = statistics.mean(dev_times)
+    ms_e2e = statistics.mean(e2e_times)
+    t_max = ms
+    t_e2e_max = ms_e2e
+    if pg is not None:
+        t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        t_max, t_e2e_max = float(t[0]), float(t[1])
+    if rank != 0:
+        return None
+
+    iters = info["iterations"]
+    upd_ms = pinfo["kernel_ms"]["update"] / max(pinfo["kernel_launches"]["update"], 1)
+    peak, peak_kind = measured_peaks()
+    # cells per launch differ across iterations; use the mean over the run
+    cells = info["n_cells"]
+    ub = update_bytes_per_launch(n, d, cells)
+    achieved = ub / (upd_ms * 1e-3) / 1e9
+    tot_k = sum(pinfo["kernel_ms"].values())
+    sample = args.cpu_sample or 2000
+    line = {
+        "metric": METRIC,
+        "value": t_max / 1000.0,
+        "unit": "s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_max,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "n": n, "d": d, "eps": eps, "iterations": iters,
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "flushed before every timed step (256 MiB write)"},
+        "e2e": {"value": t_e2e_max / 1000.0, "unit": "s", "h2d_bytes_per_step": int(n * d * 4),
+                "d2h_bytes_per_step": int(n * 4)},
+        "gpu_launches": int(info["launches"]) * args.steps,
+        "roofline": {"bound": "hbm", "kernel": "k_update", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "peak_source": peak_kind, "launch_ms": upd_ms,
+                     "launches": pinfo["kernel_launches"]["update"],
+                     "algorithmic_bytes_per_launch": ub,
+                     "share_of_kernel_time": pinfo["kernel_ms"]["update"] / tot_k if tot_k else None},
+        "kernel_ms": pinfo["kernel_ms"],
+        "stage_ms": info["stage_ms"],
+        "clocks": clocks,
+        "cpu_baseline": cpu_baseline(X, eps, iters, sample),
+    }
+    return line
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    sys.path.insert(0, str(REPO / "oracle"))
+    from eggsync import data
+
+    c = data.c5(args.seed, n=args.n)
+    X, eps = c["X"], c["eps"]
+    iters = C5_ITERATIONS or 1
+    sample = args.cpu_sample or 400
+    vals = []
+    for k in range(args.warmup + args.steps):
+        cb = cpu_baseline(X, eps, iters, sample, seed=k)
+        if k >= args.warmup:
+            vals.append(cb["value"])
+    v = statistics.mean(vals)
+    cb["value"] = v
+    n, d = X.shape
+    return {
+        "metric": METRIC, "value": v, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": v * 1000.0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded)", "impl": "reference",
+        "config": {"workload": WORKLOAD, "n": n, "d": d, "eps": eps},
+        "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    rank, local, world, pg = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            line = run_reference(args, rank, world)
+        else:
+            line = run_ours(args, rank, local, world, pg)
+        if line is not None:
+            print(json.dumps(line))
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,177 @@
+// egg_common.cuh -- shared definitions for the EGG-SynC sm_100a kernels.
+//
+// Geometry, workspace layout and the discrete decision primitives (cell ids,
+// border rule, box distance, point distance) used by every kernel.  The
+// decision primitives are written with explicit round-to-nearest intrinsics
+// so that the compiler cannot contract them; the CPU oracle uses the same
+// operation order, which makes every discrete decision (cell membership,
+// full/partial/none classification, eps tests, the convergence flag)
+// bit-identical between the two.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace egg {
+
+constexpr int kMaxDims = 64;        // generic kernels support d <= kMaxDims
+constexpr int kMaxTable = 64;       // sin/cos table half-width: |k| <= kMaxTable
+constexpr int kSortTile = 4096;     // points per radix-sort tile
+constexpr int kSortThreads = 256;
+constexpr int kHeadsBlock = 1024;   // points per block in the cell-boundary scan
+
+// Status word bits set by kernels (read by the host after the run).
+enum : int {
+    kErrNonFinite = 1,       // input holds NaN/Inf
+    kErrTable = 2,           // a cell offset fell outside the sin/cos table
+    kErrStencil = 4,
+};
+
+// Per-instance geometry, exactly as the reference computes it
+// (src/algorithms/EGG_SynC.cu:1249-1260, 1430, 563, 779, 1045).
+struct Geom {
+    int n;             // points
+    int d;             // dimensions
+    int ns;            // SoA stride (n rounded up to 32)
+    int od;            // outer grid dimensions
+    int width;         // cells per dimension
+    int n_outer;       // width^od
+    int r;             // ceil(eps / side)                 (float)
+    int r_extra;       // ceil(eps_extra / side)           (float)
+    int r_half;        // ceil((eps / 2.) / side)          (double)
+    int table_k;       // sin/cos table covers k in [-table_k, table_k]
+    float side;        // inner = outer cell side
+    float eps;
+    float eps_extra;
+    float t_eps;       // largest v with sqrtf(v) <= eps
+    float t_half;      // ... <= eps/2
+    float t_extra;     // ... <= eps_extra
+    int wpow[32];      // width^l for l < od
+};
+
+// Device workspace.  All arrays are SoA with stride g.ns where per-point or
+// per-cell with a dimension index.
+struct Work {
+    // points, in the current cell-sorted order
+    float* X;          // [d][ns] positions (current grid)
+    float* Xn;         // [d][ns] positions after the update (same order as X)
+    float* sd;         // [d][ns] sin(delta), delta = x - cell corner
+    float* md;         // [d][ns] 1 - cos(delta) (= 2 sin^2(delta/2))
+    float* qlo;        // [d][ns] eps/2-ball extremes (extra check)
+    float* qhi;        // [d][ns]
+    int* orig;         // [ns]   original index of sorted point i
+    int* orig_tmp;     // [ns]
+    int* perm;         // [ns]   radix sort output: new position -> previous position
+    int* perm_tmp;     // [ns]
+    int* cell_of;      // [ns]   cell index of sorted point i
+    // cells (index < M, M only known on the device)
+    int* cell_start;   // [ns+1]
+    int* cell_dims;    // [d][ns]
+    int* cell_outer;   // [ns]
+    float* css;        // [d][ns] sum sin(delta) per cell
+    float* csm;        // [d][ns] sum (1 - cos(delta)) per cell
+    float* cbmin;      // [d][ns] tight bounding box of the cell's points
+    float* cbmax;      // [d][ns]
+    int* outer_begin;  // [n_outer + 1]
+    // scratch for scans / sorts
+    int* hist;         // [256 * tiles]
+    int* digit_total;  // [256]
+    int* block_sums;   // [blocks]
+    double* wpart;     // [(2d values + 2d bbox) * 2 * warps] warp partials for spanning cells
+    // stencils (host-built tables)
+    int* st_delta;     // [3][st_cap] linear outer-id offset
+    signed char* st_off;  // [3][st_cap * od] per-dimension offsets
+    int st_count[3];   // entries per stencil: 0 = update (r), 1 = annulus (r_extra), 2 = ball (r_half)
+    int st_cap;
+    float* table;      // [3][2*table_k+1]: sin(ks), cos(ks), 1-cos(ks)
+    // control words
+    int* ctrl;         // [16]: see kCtrl* below
+    unsigned long long* stamps;  // [max_iter+1] globaltimer at iteration start
+    int* labels;       // [ns] output labels (original order)
+    int* iter_flags;   // [max_iter] flag after each iteration
+    int* iter_counts;  // reserved
+};
+
+enum : int {
+    kCtrlM = 0,        // number of non-empty cells
+    kCtrlFlag = 1,     // 1 = converged so far in this iteration
+    kCtrlIter = 2,     // iterations done
+    kCtrlDone = 3,     // loop finished
+    kCtrlStatus = 4,   // kErr* bits
+    kCtrlMaxIter = 5,
+    kCtrlExtraRuns = 6,   // number of extra checks run
+    kCtrlPairs = 7,       // annulus pairs examined in the last extra check
+    kCtrlClusters = 8,    // final cells holding more than one point
+};
+
+// ------------------------------------------------------------------------
+// decision primitives (identical operation order on the CPU oracle)
+// ------------------------------------------------------------------------
+__device__ __forceinline__ int cell_dim(float x, const Geom& g) {
+    int t = (int)__fdiv_rn(x, g.side);
+    if (t == g.width) t--;
+    t = t < 0 ? 0 : t;
+    t = t > g.width - 1 ? g.width - 1 : t;
+    return t;
+}
+
+// reference border rule, EGG_SynC.cu:590-596 (the +-1e-5 probes are double)
+__device__ __forceinline__ bool on_border_dim(float x, float side) {
+    int idm = (int)__ddiv_rn((double)x - 0.00001, (double)side);
+    int id = (int)__fdiv_rn(x, side);
+    int idp = (int)__ddiv_rn((double)x + 0.00001, (double)side);
+    return (id != idm) || (id != idp);
+}
+
+// reference box distance terms for one dimension, EGG_SynC.cu:613-630
+__device__ __forceinline__ void box_terms(float x, int cd, float side, float& sm, float& lg) {
+    float left = __fmul_rn((float)cd, side);
+    float right = __fmul_rn((float)(cd + 1), side);
+    left = __fsub_rn(left, x);
+    right = __fsub_rn(right, x);
+    left = __fmul_rn(left, left);
+    right = __fmul_rn(right, right);
+    if (left < right) {
+        sm = __fadd_rn(sm, left);
+        lg = __fadd_rn(lg, right);
+    } else {
+        sm = __fadd_rn(sm, right);
+        lg = __fadd_rn(lg, left);
+    }
+}
+
+__device__ __forceinline__ float dist_step(float a, float b, float acc) {
+    float diff = __fsub_rn(a, b);
+    return __fmaf_rn(diff, diff, acc);
+}
+
+// largest of |lo - x|, |hi - x| (tight bounding box, farthest face)
+__device__ __forceinline__ float far_gap(float x, float lo, float hi) {
+    float a = fabsf(__fsub_rn(lo, x));
+    float b = fabsf(__fsub_rn(hi, x));
+    return a > b ? a : b;
+}
+
+// distance from x to [lo, hi] in one dimension (0 inside)
+__device__ __forceinline__ float near_gap(float x, float lo, float hi) {
+    if (x < lo) return __fsub_rn(lo, x);
+    if (x > hi) return __fsub_rn(x, hi);
+    return 0.0f;
+}
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// first index in [b, e) whose key >= v (keys non-decreasing)
+__device__ __forceinline__ int lower_bound_i(const int* __restrict__ keys, int b, int e, int v) {
+    while (b < e) {
+        int m = (b + e) >> 1;
+        if (__ldg(keys + m) < v) b = m + 1; else e = m;
+    }
+    return b;
+}
+
+}  // namespace egg

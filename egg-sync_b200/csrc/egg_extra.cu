@@ -1,0 +1,237 @@
+// egg_extra.cu -- extra convergence check of EGG-SynC.
+//
+// Replaces kernel_float_grid_extra_check_part1_count / part1 / part2 and
+// MBR_in_eps of the reference (src/algorithms/EGG_SynC.cu:767-1203, host
+// 1425-1489).  It runs only in iterations whose update left the flag at 1
+// (both kernels return at once otherwise) and clears the flag when some pair
+// (p, q) with eps < |p - q| <= eps_extra has the per-dimension closest corner
+// of q's eps/2 group (its "MBR") within eps of p.
+//
+// The reference counts the pairs, reads the count back, allocates a pair
+// list, lists the pairs and checks each one by walking q's eps/2 group.
+// Here one pass walks the pairs and decides each one on the spot:
+//   * k_ball_bbox first records, for every point q, the extremes of its eps/2
+//     group per dimension.  When p lies outside [lo, hi] in a dimension, the
+//     group's coordinate closest to p there is the extreme itself, so the MBR
+//     is known without a walk; only dimensions where p falls inside [lo, hi]
+//     need the reference's walk (mbr_exact).
+//   * Cells are skipped wholesale with the tight bounding box of their points
+//     when no point of theirs can lie in the (eps, eps_extra] annulus.
+// Both shortcuts are exact under the shared float conventions (every
+// comparison is monotone in the coordinates).
+#include "egg_common.cuh"
+#include "egg_kernels.h"
+
+namespace egg {
+
+namespace {
+
+template <typename F>
+__device__ __forceinline__ void for_stencil_cells(const Geom& g, const Work& w, int which, int rad, const int* gi,
+                                                  int obase, int d, F&& fn) {
+    const int nst = w.st_count[which];
+    const int* st_delta = w.st_delta + (size_t)which * w.st_cap;
+    const signed char* st_off = w.st_off + (size_t)which * w.st_cap * (g.od > 0 ? g.od : 1);
+    for (int s = 0; s < nst; s++) {
+        bool inb = true;
+        for (int l = 0; l < g.od; l++) {
+            int v = gi[l] + __ldg(st_off + (size_t)s * g.od + l);
+            inb = inb && (unsigned)v < (unsigned)g.width;
+        }
+        if (!inb) continue;
+        const int o = obase + __ldg(st_delta + s);
+        int cb = __ldg(w.outer_begin + o), ce = __ldg(w.outer_begin + o + 1);
+        if (cb >= ce) continue;
+        if (g.od < d) {
+            const int* keys = w.cell_dims + (size_t)g.od * g.ns;
+            cb = lower_bound_i(keys, cb, ce, gi[g.od] - rad - 1);
+            ce = lower_bound_i(keys, cb, ce, gi[g.od] + rad + 2);
+        }
+        for (int c = cb; c < ce; c++)
+            if (!fn(c)) return;
+    }
+}
+
+// MBR_in_eps (EGG_SynC.cu:1037-1159) by the reference's walk: per dimension
+// the coordinate of q's eps/2 group with the smallest squared distance to p.
+template <int D>
+__device__ bool mbr_exact(const Geom& g, const Work& w, int qi, const float* xp) {
+    constexpr int DM = D > 0 ? D : kMaxDims;
+    const int d = D > 0 ? D : g.d;
+    float xq[DM], mbr[DM];
+    int gq[DM];
+    int obase = 0;
+    for (int l = 0; l < d; l++) {
+        xq[l] = w.X[(size_t)l * g.ns + qi];
+        mbr[l] = xq[l];
+        gq[l] = cell_dim(xq[l], g);
+        if (l < g.od) obase += gq[l] * g.wpow[l];
+    }
+    for_stencil_cells(g, w, 2, g.r_half, gq, obase, d, [&](int c) {
+        float sm2 = 0.f, lg2 = 0.f;
+        for (int l = 0; l < d; l++) box_terms(xq[l], __ldg(w.cell_dims + (size_t)l * g.ns + c), g.side, sm2, lg2);
+        if (!(sm2 <= g.t_half)) return true;
+        const int qb = __ldg(w.cell_start + c), qe = __ldg(w.cell_start + c + 1);
+        for (int r = qb; r < qe; r++) {
+            float d2 = 0.f;
+            for (int l = 0; l < d; l++) d2 = dist_step(xq[l], __ldg(w.X + (size_t)l * g.ns + r), d2);
+            if (d2 <= g.t_half) {
+                for (int l = 0; l < d; l++) {
+                    const float xr = __ldg(w.X + (size_t)l * g.ns + r);
+                    float od_ = __fsub_rn(mbr[l], xp[l]);
+                    od_ = __fmul_rn(od_, od_);
+                    float nd = __fsub_rn(xr, xp[l]);
+                    nd = __fmul_rn(nd, nd);
+                    if (nd < od_) mbr[l] = xr;
+                }
+            }
+        }
+        return true;
+    });
+    float acc = 0.f;
+    for (int l = 0; l < d; l++) acc = dist_step(mbr[l], xp[l], acc);
+    return acc <= g.t_eps;
+}
+
+}  // namespace
+
+// extremes of each point's eps/2 group (itself included)
+template <int D>
+__global__ void __launch_bounds__(128) k_ball_bbox(Geom g, Work w) {
+    constexpr int DM = D > 0 ? D : kMaxDims;
+    const int d = D > 0 ? D : g.d;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const int it = w.ctrl[kCtrlIter];
+        w.stamps[4 * it + 2] = globaltimer();
+    }
+    if (w.ctrl[kCtrlFlag] == 0) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.n) return;
+    float xq[DM], lo[DM], hi[DM];
+    int gq[DM];
+    int obase = 0;
+    for (int l = 0; l < d; l++) {
+        xq[l] = w.X[(size_t)l * g.ns + i];
+        lo[l] = hi[l] = xq[l];
+        gq[l] = cell_dim(xq[l], g);
+        if (l < g.od) obase += gq[l] * g.wpow[l];
+    }
+    for_stencil_cells(g, w, 2, g.r_half, gq, obase, d, [&](int c) {
+        float sm2 = 0.f, lg2 = 0.f;
+        for (int l = 0; l < d; l++) box_terms(xq[l], __ldg(w.cell_dims + (size_t)l * g.ns + c), g.side, sm2, lg2);
+        if (!(sm2 <= g.t_half)) return true;
+        // all of the cell's points inside the eps/2 ball?
+        float far2 = 0.f;
+        for (int l = 0; l < d; l++) {
+            const float a = far_gap(xq[l], __ldg(w.cbmin + (size_t)l * g.ns + c), __ldg(w.cbmax + (size_t)l * g.ns + c));
+            far2 = __fmaf_rn(a, a, far2);
+        }
+        if (far2 <= g.t_half) {
+            for (int l = 0; l < d; l++) {
+                lo[l] = fminf(lo[l], __ldg(w.cbmin + (size_t)l * g.ns + c));
+                hi[l] = fmaxf(hi[l], __ldg(w.cbmax + (size_t)l * g.ns + c));
+            }
+            return true;
+        }
+        const int qb = __ldg(w.cell_start + c), qe = __ldg(w.cell_start + c + 1);
+        for (int r = qb; r < qe; r++) {
+            float d2 = 0.f;
+            for (int l = 0; l < d; l++) d2 = dist_step(xq[l], __ldg(w.X + (size_t)l * g.ns + r), d2);
+            if (d2 <= g.t_half)
+                for (int l = 0; l < d; l++) {
+                    const float v = __ldg(w.X + (size_t)l * g.ns + r);
+                    lo[l] = fminf(lo[l], v);
+                    hi[l] = fmaxf(hi[l], v);
+                }
+        }
+        return true;
+    });
+    for (int l = 0; l < d; l++) {
+        w.qlo[(size_t)l * g.ns + i] = lo[l];
+        w.qhi[(size_t)l * g.ns + i] = hi[l];
+    }
+}
+
+template <int D>
+__global__ void __launch_bounds__(128) k_annulus(Geom g, Work w) {
+    constexpr int DM = D > 0 ? D : kMaxDims;
+    const int d = D > 0 ? D : g.d;
+    volatile int* flag = w.ctrl + kCtrlFlag;
+    if (*flag == 0) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.n) return;
+    float xp[DM];
+    int gp[DM];
+    int obase = 0;
+    for (int l = 0; l < d; l++) {
+        xp[l] = w.X[(size_t)l * g.ns + i];
+        gp[l] = cell_dim(xp[l], g);
+        if (l < g.od) obase += gp[l] * g.wpow[l];
+    }
+    int pairs = 0;
+    bool violated = false;
+    for_stencil_cells(g, w, 1, g.r_extra, gp, obase, d, [&](int c) {
+        if (*flag == 0) return false;
+        float sm2 = 0.f, lg2 = 0.f;
+        for (int l = 0; l < d; l++) box_terms(xp[l], __ldg(w.cell_dims + (size_t)l * g.ns + c), g.side, sm2, lg2);
+        const bool included = sm2 <= g.t_extra;
+        const bool fully = lg2 <= g.t_eps;
+        if (!included || fully) return true;
+        float near2 = 0.f, far2 = 0.f;
+        for (int l = 0; l < d; l++) {
+            const float lo = __ldg(w.cbmin + (size_t)l * g.ns + c), hi = __ldg(w.cbmax + (size_t)l * g.ns + c);
+            const float a = near_gap(xp[l], lo, hi), b = far_gap(xp[l], lo, hi);
+            near2 = __fmaf_rn(a, a, near2);
+            far2 = __fmaf_rn(b, b, far2);
+        }
+        if (near2 > g.t_extra || far2 <= g.t_eps) return true;
+        const int qb = __ldg(w.cell_start + c), qe = __ldg(w.cell_start + c + 1);
+        for (int q = qb; q < qe; q++) {
+            float d2 = 0.f;
+            for (int l = 0; l < d; l++) d2 = dist_step(xp[l], __ldg(w.X + (size_t)l * g.ns + q), d2);
+            if (!(d2 > g.t_eps && d2 <= g.t_extra)) continue;
+            pairs++;
+            bool resolved = true;
+            float acc = 0.f;
+            for (int l = 0; l < d; l++) {
+                const float lo = __ldg(w.qlo + (size_t)l * g.ns + q), hi = __ldg(w.qhi + (size_t)l * g.ns + q);
+                float m;
+                if (xp[l] >= hi) m = hi;
+                else if (xp[l] <= lo) m = lo;
+                else { resolved = false; break; }
+                acc = dist_step(m, xp[l], acc);
+            }
+            const bool in_eps = resolved ? (acc <= g.t_eps) : mbr_exact<D>(g, w, q, xp);
+            if (in_eps) {
+                violated = true;
+                *flag = 0;
+                return false;
+            }
+        }
+        return true;
+    });
+    if (pairs) atomicAdd(w.ctrl + kCtrlPairs, pairs);
+    (void)violated;
+}
+
+#define EGG_DISPATCH_D(d, KERNEL, ...)                \
+    switch (d) {                                      \
+        case 1: KERNEL<1> __VA_ARGS__; break;         \
+        case 2: KERNEL<2> __VA_ARGS__; break;         \
+        case 3: KERNEL<3> __VA_ARGS__; break;         \
+        case 4: KERNEL<4> __VA_ARGS__; break;         \
+        case 5: KERNEL<5> __VA_ARGS__; break;         \
+        case 6: KERNEL<6> __VA_ARGS__; break;         \
+        case 8: KERNEL<8> __VA_ARGS__; break;         \
+        case 16: KERNEL<16> __VA_ARGS__; break;       \
+        default: KERNEL<0> __VA_ARGS__; break;        \
+    }
+
+void launch_extra_check(const Geom& g, const Work& w, cudaStream_t st) {
+    const int threads = 128;
+    const int blocks = (g.n + threads - 1) / threads;
+    EGG_DISPATCH_D(g.d, k_ball_bbox, <<<blocks, threads, 0, st>>>(g, w));
+    EGG_DISPATCH_D(g.d, k_annulus, <<<blocks, threads, 0, st>>>(g, w));
+}
+
+}  // namespace egg

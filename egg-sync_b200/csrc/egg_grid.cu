@@ -1,0 +1,520 @@
+// egg_grid.cu -- double-grid spatial index for EGG-SynC on sm_100a.
+//
+// Replaces build_the_grid + kernel_inner_grid_stats of the reference
+// (src/algorithms/EGG_SynC.cu:78-341, 344-366) and its recursive
+// Brent-Kung scan (src/utils/GPU_utils.cu:12-238).
+//
+// The reference keeps a dense outer grid over the first `od` dimensions and,
+// inside each outer cell, a list of inner cells found by a linear search.
+// Here the same structure is obtained by one stable LSD radix sort of the
+// points on their cell tuple, ordered (outer id, g_od, ..., g_{d-1}), so:
+//   * every inner cell is a contiguous run of sorted points,
+//   * the inner cells of one outer cell are contiguous and sorted by g_od
+//     (the update kernel binary-searches that dimension),
+//   * outer cell o owns cells [outer_begin[o], outer_begin[o+1]).
+// The sort never materialises keys: each pass recomputes one dimension's
+// cell digit from the positions through the current permutation.  All
+// passes are stable and run in a fixed order, so the whole index (and the
+// cell sums below) is bit-reproducible from run to run.
+#include "egg_common.cuh"
+#include "egg_kernels.h"
+
+namespace egg {
+
+namespace {
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// block-wide exclusive scan of one int per thread (blockDim.x <= 1024)
+__device__ int block_exclusive_scan(int v, int* total) {
+    __shared__ int warp_sums[33];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_sums[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        int s = lane < nw ? warp_sums[lane] : 0;
+        int si = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, si, o);
+            if (lane >= o) si += t;
+        }
+        if (lane < nw) warp_sums[lane] = si - s;
+        if (lane == 31) warp_sums[32] = si;  // lanes >= nw add 0: lane 31 holds the total
+    }
+    __syncthreads();
+    int excl = incl - v + warp_sums[wid];
+    if (total) *total = warp_sums[32];
+    __syncthreads();
+    return excl;
+}
+
+__device__ __forceinline__ int digit_of(const Geom& g, const float* __restrict__ Xs, int j, int dim, int shift) {
+    float x = __ldg(Xs + (size_t)dim * g.ns + j);
+    return (cell_dim(x, g) >> shift) & 255;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// radix sort pass: tile histograms
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kSortThreads) k_radix_hist(Geom g, const float* __restrict__ Xs,
+                                                             const int* __restrict__ pin, int first, int dim,
+                                                             int shift, int* __restrict__ hist, int tiles) {
+    __shared__ int h[256];
+    for (int t = threadIdx.x; t < 256; t += blockDim.x) h[t] = 0;
+    __syncthreads();
+    const int base = blockIdx.x * kSortTile;
+    const int end = min(base + kSortTile, g.n);
+    for (int i = base + threadIdx.x; i < end; i += blockDim.x) {
+        int j = first ? i : __ldg(pin + i);
+        int dg = digit_of(g, Xs, j, dim, shift);
+        unsigned act = __activemask();
+        unsigned peers = __match_any_sync(act, dg);
+        if ((peers & lanemask_lt()) == 0) atomicAdd(&h[dg], __popc(peers));
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < 256; t += blockDim.x) hist[(size_t)t * tiles + blockIdx.x] = h[t];
+}
+
+// per-digit exclusive scan over tiles (one block per digit)
+__global__ void __launch_bounds__(256) k_radix_scan(int* __restrict__ hist, int tiles, int* __restrict__ digit_total) {
+    int* h = hist + (size_t)blockIdx.x * tiles;
+    const int per = (tiles + blockDim.x - 1) / blockDim.x;
+    const int b = threadIdx.x * per;
+    const int e = min(b + per, tiles);
+    int s = 0;
+    for (int k = b; k < e; k++) s += h[k];
+    int total;
+    int run = block_exclusive_scan(s, &total);
+    for (int k = b; k < e; k++) {
+        int v = h[k];
+        h[k] = run;
+        run += v;
+    }
+    if (threadIdx.x == 0) digit_total[blockIdx.x] = total;
+}
+
+// stable scatter of one tile
+__global__ void __launch_bounds__(kSortThreads) k_radix_scatter(Geom g, const float* __restrict__ Xs,
+                                                                const int* __restrict__ pin, int first, int dim,
+                                                                int shift, const int* __restrict__ hist,
+                                                                const int* __restrict__ digit_total, int tiles,
+                                                                int* __restrict__ pout) {
+    constexpr int kWarps = kSortThreads / 32;
+    __shared__ int base[256];
+    __shared__ int run[256];
+    __shared__ int wcnt[kWarps][256];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    {
+        int v = digit_total[tid];
+        int db = block_exclusive_scan(v, nullptr);
+        base[tid] = db + hist[(size_t)tid * tiles + blockIdx.x];
+        run[tid] = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; w++) wcnt[w][tid] = 0;
+    }
+    __syncthreads();
+    const int tile0 = blockIdx.x * kSortTile;
+    for (int round = 0; round < kSortTile / kSortThreads; round++) {
+        const int i = tile0 + round * kSortThreads + tid;
+        if (tile0 + round * kSortThreads >= g.n) break;  // uniform across the block
+        const bool valid = i < g.n;
+        int j = 0, dg = 0;
+        if (valid) {
+            j = first ? i : __ldg(pin + i);
+            dg = digit_of(g, Xs, j, dim, shift);
+        }
+        unsigned peers = __match_any_sync(0xffffffffu, valid ? dg : 256 + lane);
+        int rank = __popc(peers & lanemask_lt());
+        if (valid && rank == 0) wcnt[wid][dg] = __popc(peers);
+        __syncthreads();
+        {
+            int r = run[tid];
+#pragma unroll
+            for (int w = 0; w < kWarps; w++) {
+                int c = wcnt[w][tid];
+                wcnt[w][tid] = r;
+                r += c;
+            }
+            run[tid] = r;
+        }
+        __syncthreads();
+        if (valid) pout[base[dg] + wcnt[wid][dg] + rank] = j;
+        __syncthreads();
+#pragma unroll
+        for (int w = 0; w < kWarps; w++) wcnt[w][tid] = 0;
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// gather into the new order and count cell heads per block
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(kHeadsBlock) k_gather_heads(Geom g, Work w, int identity) {
+    const int d = D > 0 ? D : g.d;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int head = 0;
+    if (i < g.n) {
+        const int j = identity ? i : __ldg(w.perm + i);
+        const int jp = i > 0 ? (identity ? i - 1 : __ldg(w.perm + i - 1)) : 0;
+        head = (i == 0);
+        for (int l = 0; l < d; l++) {
+            float x = __ldg(w.Xn + (size_t)l * g.ns + j);
+            w.X[(size_t)l * g.ns + i] = x;
+            if (i > 0) {
+                float xp = __ldg(w.Xn + (size_t)l * g.ns + jp);
+                head |= (cell_dim(x, g) != cell_dim(xp, g));
+            }
+        }
+        w.orig_tmp[i] = __ldg(w.orig + j);
+    }
+    int total;
+    block_exclusive_scan(head, &total);
+    if (threadIdx.x == 0) w.block_sums[blockIdx.x] = total;
+}
+
+// single-block exclusive scan of the per-block head counts; M = total
+__global__ void __launch_bounds__(1024) k_scan_block_sums(int* __restrict__ bs, int nb, int* __restrict__ ctrl) {
+    const int per = (nb + blockDim.x - 1) / blockDim.x;
+    const int b = threadIdx.x * per;
+    const int e = min(b + per, nb);
+    int s = 0;
+    for (int k = b; k < e; k++) s += bs[k];
+    int total;
+    int run = block_exclusive_scan(s, &total);
+    for (int k = b; k < e; k++) {
+        int v = bs[k];
+        bs[k] = run;
+        run += v;
+    }
+    if (threadIdx.x == 0) ctrl[kCtrlM] = total;
+}
+
+template <int D>
+__global__ void __launch_bounds__(kHeadsBlock) k_heads_finalize(Geom g, Work w) {
+    const int d = D > 0 ? D : g.d;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int head = 0;
+    if (i < g.n) {
+        head = (i == 0);
+        if (i > 0)
+            for (int l = 0; l < d && !head; l++)
+                head = cell_dim(w.X[(size_t)l * g.ns + i], g) != cell_dim(w.X[(size_t)l * g.ns + i - 1], g);
+    }
+    int excl = block_exclusive_scan(head, nullptr) + w.block_sums[blockIdx.x];
+    if (i < g.n) {
+        const int c = excl + head - 1;
+        w.cell_of[i] = c;
+        w.orig[i] = w.orig_tmp[i];
+        if (head) {
+            w.cell_start[c] = i;
+            int outer = 0;
+            for (int l = 0; l < d; l++) {
+                int gl = cell_dim(w.X[(size_t)l * g.ns + i], g);
+                w.cell_dims[(size_t)l * g.ns + c] = gl;
+                if (l < g.od) outer += gl * g.wpow[l];
+            }
+            w.cell_outer[c] = outer;
+        }
+        if (i == g.n - 1) w.cell_start[c + 1] = g.n;
+    }
+}
+
+// outer_begin[o] = first cell whose outer id >= o, o in [0, n_outer]
+__global__ void k_outer_ranges(Geom g, Work w) {
+    const int M = w.ctrl[kCtrlM];
+    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o <= g.n_outer; o += gridDim.x * blockDim.x)
+        w.outer_begin[o] = lower_bound_i(w.cell_outer, 0, M, o);
+}
+
+// ---------------------------------------------------------------------------
+// per-cell sums of sin(delta) and 1 - cos(delta), delta = x - cell corner,
+// plus the tight bounding box of each cell's points
+// ---------------------------------------------------------------------------
+namespace {
+
+struct TwoSum {
+    float hi, lo;
+};
+
+__device__ __forceinline__ TwoSum ts_add(TwoSum a, TwoSum b) {
+    float s = __fadd_rn(a.hi, b.hi);
+    float bb = __fsub_rn(s, a.hi);
+    float err = __fadd_rn(__fsub_rn(a.hi, __fsub_rn(s, bb)), __fsub_rn(b.hi, bb));
+    return {s, __fadd_rn(__fadd_rn(a.lo, b.lo), err)};
+}
+
+// warp-partial layout: ((field * d + l) * 2 + rec) * warps + warp, field in
+// {sum sin, sum 1-cos, min, max}, rec 0 = segment holding lane 0, 1 = lane 31
+__device__ __forceinline__ size_t wp_idx(int field, int l, int d, int rec, int nw, int warp) {
+    return ((size_t)(field * d + l) * 2 + rec) * nw + warp;
+}
+
+}  // namespace
+
+template <int D>
+__global__ void __launch_bounds__(256) k_cell_sums(Geom g, Work w) {
+    constexpr int DM = D > 0 ? D : kMaxDims;
+    const int d = D > 0 ? D : g.d;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int warp = i >> 5;
+    const int nw = (g.n + 31) >> 5;
+    if ((i & ~31) >= g.n) return;  // whole warp beyond n
+    const bool valid = i < g.n;
+    const int c = valid ? w.cell_of[i] : 0x7fffffff - lane;
+    const int cnext = __shfl_down_sync(0xffffffffu, c, 1);
+    const int cprev = __shfl_up_sync(0xffffffffu, c, 1);
+    const bool seg_end = valid && (lane == 31 || cnext != c);
+    const bool seg_start = valid && (lane == 0 || cprev != c);
+    (void)seg_start;
+    const int wb = i & ~31;
+    int cs = 0, ce = 0;
+    if (seg_end) {
+        cs = w.cell_start[c];
+        ce = w.cell_start[c + 1];
+    }
+    const bool complete = seg_end && cs >= wb && ce <= wb + 32;
+    // segment start lane: for the record of the first segment
+    for (int l = 0; l < d; l++) {
+        float s = 0.f, m = 0.f, x = 0.f;
+        if (valid) {
+            x = w.X[(size_t)l * g.ns + i];
+            int cd = w.cell_dims[(size_t)l * g.ns + c];
+            float corner = __fmul_rn((float)cd, g.side);
+            float delta = __fsub_rn(x, corner);
+            float sh, ch;
+            sincosf(0.5f * delta, &sh, &ch);
+            s = 2.0f * sh * ch;
+            m = 2.0f * sh * sh;
+            w.sd[(size_t)l * g.ns + i] = s;
+            w.md[(size_t)l * g.ns + i] = m;
+        }
+        TwoSum vs{s, 0.f}, vm{m, 0.f};
+        float mn = x, mx = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            TwoSum us{__shfl_up_sync(0xffffffffu, vs.hi, o), __shfl_up_sync(0xffffffffu, vs.lo, o)};
+            TwoSum um{__shfl_up_sync(0xffffffffu, vm.hi, o), __shfl_up_sync(0xffffffffu, vm.lo, o)};
+            float umn = __shfl_up_sync(0xffffffffu, mn, o);
+            float umx = __shfl_up_sync(0xffffffffu, mx, o);
+            int uc = __shfl_up_sync(0xffffffffu, c, o);
+            if (lane >= o && uc == c) {
+                vs = ts_add(us, vs);
+                vm = ts_add(um, vm);
+                mn = fminf(mn, umn);
+                mx = fmaxf(mx, umx);
+            }
+        }
+        if (complete) {
+            w.css[(size_t)l * g.ns + c] = __fadd_rn(vs.hi, vs.lo);
+            w.csm[(size_t)l * g.ns + c] = __fadd_rn(vm.hi, vm.lo);
+            w.cbmin[(size_t)l * g.ns + c] = mn;
+            w.cbmax[(size_t)l * g.ns + c] = mx;
+        } else if (seg_end) {
+            // partial of a cell spanning several warps: rec 0 = segment holding
+            // lane 0 (continues from the previous warp), rec 1 = segment holding
+            // lane 31 (continues into the next warp); a warp inside one cell
+            // writes both.
+            const double S = (double)vs.hi + (double)vs.lo;
+            const double Mm = (double)vm.hi + (double)vm.lo;
+            if (cs < wb) {
+                w.wpart[wp_idx(0, l, d, 0, nw, warp)] = S;
+                w.wpart[wp_idx(1, l, d, 0, nw, warp)] = Mm;
+                w.wpart[wp_idx(2, l, d, 0, nw, warp)] = mn;
+                w.wpart[wp_idx(3, l, d, 0, nw, warp)] = mx;
+            }
+            if (ce > wb + 32) {
+                w.wpart[wp_idx(0, l, d, 1, nw, warp)] = S;
+                w.wpart[wp_idx(1, l, d, 1, nw, warp)] = Mm;
+                w.wpart[wp_idx(2, l, d, 1, nw, warp)] = mn;
+                w.wpart[wp_idx(3, l, d, 1, nw, warp)] = mx;
+            }
+        }
+    }
+    (void)DM;
+}
+
+// Cells spanning more than one warp (the heavily populated ones): combine the
+// warp partials in FP64 in a fixed order.  One warp per 32 cells.
+__global__ void __launch_bounds__(256) k_cell_sums_fix(Geom g, Work w) {
+    const int M = w.ctrl[kCtrlM];
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int c0 = gw * 32;
+    if (c0 >= M) return;
+    const int nw = (g.n + 31) >> 5;
+    const int c = c0 + lane;
+    int cs = 0, ce = 0;
+    bool span = false;
+    if (c < M) {
+        cs = w.cell_start[c];
+        ce = w.cell_start[c + 1];
+        span = (cs >> 5) != ((ce - 1) >> 5);
+    }
+    unsigned todo = __ballot_sync(0xffffffffu, span);
+    while (todo) {
+        const int src = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const int cc = c0 + src;
+        const int scs = __shfl_sync(0xffffffffu, cs, src);
+        const int sce = __shfl_sync(0xffffffffu, ce, src);
+        const int wh = scs >> 5, wt = (sce - 1) >> 5;
+        for (int l = 0; l < g.d; l++) {
+            double S = 0.0, Mm = 0.0, mn = 1e300, mx = -1e300;
+            for (int k = wh + lane; k <= wt; k += 32) {
+                const int rec = (k == wh) ? 1 : 0;
+                S += w.wpart[wp_idx(0, l, g.d, rec, nw, k)];
+                Mm += w.wpart[wp_idx(1, l, g.d, rec, nw, k)];
+                mn = fmin(mn, w.wpart[wp_idx(2, l, g.d, rec, nw, k)]);
+                mx = fmax(mx, w.wpart[wp_idx(3, l, g.d, rec, nw, k)]);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                S += __shfl_xor_sync(0xffffffffu, S, o);
+                Mm += __shfl_xor_sync(0xffffffffu, Mm, o);
+                mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+                mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            }
+            if (lane == 0) {
+                w.css[(size_t)l * g.ns + cc] = (float)S;
+                w.csm[(size_t)l * g.ns + cc] = (float)Mm;
+                w.cbmin[(size_t)l * g.ns + cc] = (float)mn;
+                w.cbmax[(size_t)l * g.ns + cc] = (float)mx;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// misc: input transpose, labels
+// ---------------------------------------------------------------------------
+__global__ void k_transpose_in(Geom g, Work w, const float* __restrict__ x_aos) {
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < (size_t)g.n * g.d;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const int p = (int)(t / g.d), l = (int)(t % g.d);
+        float v = x_aos[t];
+        if (!isfinite(v)) atomicOr(w.ctrl + kCtrlStatus, kErrNonFinite);
+        w.Xn[(size_t)l * g.ns + p] = v;
+        if (l == 0) w.orig[p] = p;
+    }
+}
+
+// positions of the sorted points back to original order (row-major n x d)
+__global__ void k_unsort_positions(Geom g, Work w, const float* __restrict__ src, float* __restrict__ out) {
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < (size_t)g.n * g.d;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(t % g.n), l = (int)(t / g.n);
+        out[(size_t)w.orig[i] * g.d + l] = src[(size_t)l * g.ns + i];
+    }
+}
+
+// GPU_synCluster_float_grid semantics, EGG_SynC.cu:1205-1227: the compacted
+// cell index when the cell holds more than one point, else -1.
+__global__ void k_labels(Geom g, Work w, int* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+        const int c = w.cell_of[i];
+        const int cs = w.cell_start[c];
+        const int cnt = w.cell_start[c + 1] - cs;
+        out[w.orig[i]] = cnt > 1 ? c : -1;
+        if (i == cs && cnt > 1) atomicAdd(w.ctrl + kCtrlClusters, 1);
+    }
+}
+
+__global__ void k_unsort_int(Geom g, Work w, const int* __restrict__ src, int* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x)
+        out[w.orig[i]] = src[i];
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+#define EGG_DISPATCH_D(d, KERNEL, ...)                \
+    switch (d) {                                      \
+        case 1: KERNEL<1> __VA_ARGS__; break;         \
+        case 2: KERNEL<2> __VA_ARGS__; break;         \
+        case 3: KERNEL<3> __VA_ARGS__; break;         \
+        case 4: KERNEL<4> __VA_ARGS__; break;         \
+        case 5: KERNEL<5> __VA_ARGS__; break;         \
+        case 6: KERNEL<6> __VA_ARGS__; break;         \
+        case 8: KERNEL<8> __VA_ARGS__; break;         \
+        case 16: KERNEL<16> __VA_ARGS__; break;       \
+        default: KERNEL<0> __VA_ARGS__; break;        \
+    }
+
+void launch_sort(const Geom& g, const Work& w, const SortPlan& plan, cudaStream_t st) {
+    const int tiles = (g.n + kSortTile - 1) / kSortTile;
+    const int* pin = nullptr;
+    int* bufs[2] = {w.perm, w.perm_tmp};
+    // the last pass must land in w.perm
+    int out = (plan.count % 2 == 1) ? 0 : 1;
+    for (int p = 0; p < plan.count; p++) {
+        const int first = (p == 0);
+        int* pout = bufs[out];
+        k_radix_hist<<<tiles, kSortThreads, 0, st>>>(g, w.Xn, pin, first, plan.dim[p], plan.shift[p], w.hist, tiles);
+        k_radix_scan<<<256, 256, 0, st>>>(w.hist, tiles, w.digit_total);
+        k_radix_scatter<<<tiles, kSortThreads, 0, st>>>(g, w.Xn, pin, first, plan.dim[p], plan.shift[p], w.hist,
+                                                        w.digit_total, tiles, pout);
+        pin = pout;
+        out ^= 1;
+    }
+}
+
+void launch_build(const Geom& g, const Work& w, const SortPlan& plan, cudaStream_t st) {
+    const int identity = plan.count == 0;
+    if (!identity) launch_sort(g, w, plan, st);
+    const int nb = (g.n + kHeadsBlock - 1) / kHeadsBlock;
+    EGG_DISPATCH_D(g.d, k_gather_heads, <<<nb, kHeadsBlock, 0, st>>>(g, w, identity));
+    k_scan_block_sums<<<1, 1024, 0, st>>>(w.block_sums, nb, w.ctrl);
+    EGG_DISPATCH_D(g.d, k_heads_finalize, <<<nb, kHeadsBlock, 0, st>>>(g, w));
+    k_outer_ranges<<<(g.n_outer + 1 + 255) / 256, 256, 0, st>>>(g, w);
+}
+
+void launch_cell_sums(const Geom& g, const Work& w, cudaStream_t st) {
+    const int blocks = (g.n + 255) / 256;
+    EGG_DISPATCH_D(g.d, k_cell_sums, <<<blocks, 256, 0, st>>>(g, w));
+    const int fix_warps = (g.n + 31) / 32;
+    k_cell_sums_fix<<<(fix_warps * 32 + 255) / 256, 256, 0, st>>>(g, w);
+}
+
+void launch_transpose_in(const Geom& g, const Work& w, const float* x, cudaStream_t st) {
+    size_t tot = (size_t)g.n * g.d;
+    int blocks = (int)((tot + 255) / 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_transpose_in<<<blocks, 256, 0, st>>>(g, w, x);
+}
+
+void launch_unsort_positions(const Geom& g, const Work& w, const float* src, float* out, cudaStream_t st) {
+    size_t tot = (size_t)g.n * g.d;
+    int blocks = (int)((tot + 255) / 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_unsort_positions<<<blocks, 256, 0, st>>>(g, w, src, out);
+}
+
+void launch_unsort_int(const Geom& g, const Work& w, const int* src, int* out, cudaStream_t st) {
+    int blocks = (g.n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_unsort_int<<<blocks, 256, 0, st>>>(g, w, src, out);
+}
+
+void launch_labels(const Geom& g, const Work& w, int* out, cudaStream_t st) {
+    int blocks = (g.n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_labels<<<blocks, 256, 0, st>>>(g, w, out);
+}
+
+}  // namespace egg

@@ -1,0 +1,717 @@
+// egg_host.cu -- host orchestration and C ABI of libeggsync.so.
+//
+// Replaces the host driver of the reference, EGG_SynC(float*, n, d, eps)
+// (src/algorithms/EGG_SynC.cu:1229-1601).  Differences in how, not what:
+//   * one device workspace per GPU, allocated once and grown on demand
+//     (the reference allocates ~20 buffers per call and cudaMallocs inside
+//     every scan and every extra check);
+//   * the whole while-loop runs on the device: one CUDA graph whose
+//     conditional while node repeats the iteration body until the
+//     convergence flag (or the iteration cap) stops it, so there is no host
+//     synchronisation between iterations (the reference has at least seven
+//     device syncs and two to four readbacks per iteration);
+//   * stage and iteration times come from %globaltimer stamps written by the
+//     kernels, in the reference's six stage slots;
+//   * failures are returned as status codes (the reference calls exit()).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "eggsync.h"
+#include "egg_common.cuh"
+#include "egg_kernels.h"
+
+namespace egg {
+
+namespace {
+
+thread_local std::string g_last_error;
+std::mutex g_mutex;
+
+struct CudaError {
+    cudaError_t code;
+    std::string where;
+};
+
+#define EGG_CHECK(call)                                                              \
+    do {                                                                             \
+        cudaError_t _e = (call);                                                     \
+        if (_e != cudaSuccess) throw CudaError{_e, std::string(#call) + " @" +       \
+                                                     std::to_string(__LINE__)};      \
+    } while (0)
+
+struct ArgError {
+    int status;
+    std::string msg;
+};
+
+// ------------------------------------------------------------------------
+// geometry, stencils, tables
+// ------------------------------------------------------------------------
+float sq_threshold(float e) {
+    float t = e * e;
+    while (t > 0.0f && sqrtf(t) > e) t = nextafterf(t, 0.0f);
+    for (;;) {
+        float u = nextafterf(t, INFINITY);
+        if (sqrtf(u) <= e) t = u; else break;
+    }
+    return t;
+}
+
+// EGG_SynC.cu:1249-1260, 1430, 563, 779, 1045
+Geom make_geom(int64_t n64, int d, float eps) {
+    if (n64 < 1 || n64 > (int64_t)0x7ffffff0 / 4) throw ArgError{EGG_ERR_ARG, "n out of range"};
+    if (d < 1 || d > kMaxDims) throw ArgError{EGG_ERR_ARG, "d must be in [1, 64]"};
+    if (!(eps > 0.0f) || !std::isfinite(eps)) throw ArgError{EGG_ERR_ARG, "eps must be positive and finite"};
+    const int n = (int)n64;
+    Geom g;
+    memset(&g, 0, sizeof(g));
+    g.n = n;
+    g.d = d;
+    g.ns = (n + 31) & ~31;
+    g.eps = eps;
+    g.side = (float)sqrt(pow((double)eps / 2., 2.) / (double)d);
+    g.width = (int)(1.0f / g.side);
+    if (g.width < 2) throw ArgError{EGG_ERR_GEOMETRY, "eps too large: fewer than 2 cells per dimension"};
+    if (g.width > 65535) throw ArgError{EGG_ERR_GEOMETRY, "eps too small: more than 65535 cells per dimension"};
+    int od = (int)(log((double)n) / log((double)g.width));
+    od = std::min(d, std::max(od, 0));
+    g.od = od;
+    const double no = pow((double)g.width, (double)od);
+    if (no > 2.0e9) throw ArgError{EGG_ERR_GEOMETRY, "outer grid too large"};
+    g.n_outer = (int)no;
+    int p = 1;
+    for (int l = 0; l < od && l < 32; l++) {
+        g.wpow[l] = p;
+        p *= g.width;
+    }
+    g.r = (int)ceilf(eps / g.side);
+    g.eps_extra = (float)((double)(2.0f * eps) - (double)eps * sqrt(15. / 16.) + (double)eps / 2. -
+                          sin((double)eps / 2.));
+    g.r_extra = (int)ceilf(g.eps_extra / g.side);
+    g.r_half = (int)ceil(((double)eps / 2.) / (double)g.side);
+    g.t_eps = sq_threshold(eps);
+    g.t_half = sq_threshold(eps / 2.0f);
+    g.t_extra = sq_threshold(g.eps_extra);
+    g.table_k = std::max(g.r, std::max(g.r_extra, g.r_half)) + 2;
+    if (g.table_k > kMaxTable) throw ArgError{EGG_ERR_GEOMETRY, "stencil radius too large"};
+    return g;
+}
+
+SortPlan make_plan(const Geom& g) {
+    SortPlan P;
+    auto add_dim = [&](int l) {
+        P.dim[P.count] = l;
+        P.shift[P.count] = 0;
+        P.count++;
+        if (g.width > 256) {
+            P.dim[P.count] = l;
+            P.shift[P.count] = 8;
+            P.count++;
+        }
+    };
+    // least significant first: g_{d-1}, ..., g_od, then g_0, ..., g_{od-1}
+    for (int l = g.d - 1; l >= g.od; l--) add_dim(l);
+    for (int l = 0; l < g.od; l++) add_dim(l);
+    return P;
+}
+
+struct Stencil {
+    std::vector<int> delta;
+    std::vector<signed char> off;
+};
+
+Stencil make_stencil(const Geom& g, int rad) {
+    Stencil S;
+    const int od = g.od;
+    if (od == 0) {
+        S.delta.push_back(0);
+        return S;
+    }
+    double cnt = pow(2.0 * rad + 1.0, (double)od);
+    if (cnt > 4.0e6 || rad > 127) throw ArgError{EGG_ERR_GEOMETRY, "stencil too large"};
+    std::vector<int> idx(od, -rad);
+    for (;;) {
+        int delta = 0;
+        for (int l = 0; l < od; l++) {
+            delta += idx[l] * g.wpow[l];
+            S.off.push_back((signed char)idx[l]);
+        }
+        S.delta.push_back(delta);
+        int l = 0;
+        idx[0]++;
+        while (l < od - 1 && idx[l] > rad) {
+            idx[l] = -rad;
+            l++;
+            idx[l]++;
+        }
+        if (idx[od - 1] > rad) break;
+    }
+    return S;
+}
+
+size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
+
+// ------------------------------------------------------------------------
+// per-device instance: workspace, stream, graph
+// ------------------------------------------------------------------------
+struct Instance {
+    int dev = -1;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev[6] = {};
+    cudaEvent_t prof[8] = {};              // kernel-group timing (opts.profile)
+    void* base = nullptr;
+    size_t cap = 0;
+    int* h_ctrl = nullptr;                 // pinned mirror of ctrl
+    unsigned long long* h_stamps = nullptr;
+    int h_stamps_cap = 0;
+    // current layout
+    Geom g;
+    Work w;
+    SortPlan plan;
+    float* xin = nullptr;                  // staging for host input (n*d)
+    int max_iter = 0;
+    size_t used = 0;
+    // graph cache
+    cudaGraphExec_t exec = nullptr;
+    std::vector<char> graph_key;
+    bool graph_failed = false;
+};
+
+std::map<int, Instance*> g_inst;
+
+void destroy_graph(Instance& I) {
+    if (I.exec) cudaGraphExecDestroy(I.exec);
+    I.exec = nullptr;
+    I.graph_key.clear();
+}
+
+Instance& instance() {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) throw CudaError{e, "cudaGetDevice"};
+    auto it = g_inst.find(dev);
+    if (it != g_inst.end()) return *it->second;
+    Instance* I = new Instance();
+    I->dev = dev;
+    EGG_CHECK(cudaStreamCreateWithFlags(&I->st, cudaStreamNonBlocking));
+    for (auto& e2 : I->ev) EGG_CHECK(cudaEventCreate(&e2));
+    EGG_CHECK(cudaMallocHost((void**)&I->h_ctrl, 16 * sizeof(int)));
+    g_inst[dev] = I;
+    return *I;
+}
+
+// Lay out the workspace for geometry g (allocating or growing it) and
+// upload the stencils and tables.
+void prepare(Instance& I, const Geom& g, int max_iter) {
+    const int d = g.d;
+    const size_t ns = (size_t)g.ns;
+    const int tiles = (g.n + kSortTile - 1) / kSortTile;
+    const int nb = (g.n + kHeadsBlock - 1) / kHeadsBlock;
+    const int nw = (g.n + 31) / 32;
+    Stencil st[3] = {make_stencil(g, g.r), make_stencil(g, g.r_extra), make_stencil(g, g.r_half)};
+    int st_cap = 1;
+    for (auto& s : st) st_cap = std::max(st_cap, (int)s.delta.size());
+    const int odp = std::max(g.od, 1);
+    const int TW = 2 * g.table_k + 1;
+
+    size_t off = 0;
+    std::vector<std::pair<void**, size_t>> plan;
+    Work w;
+    memset(&w, 0, sizeof(w));
+    float* xin = nullptr;
+    auto add = [&](void** p, size_t bytes) { plan.push_back({p, bytes}); };
+    add((void**)&w.X, 4 * d * ns);
+    add((void**)&w.Xn, 4 * d * ns);
+    add((void**)&w.sd, 4 * d * ns);
+    add((void**)&w.md, 4 * d * ns);
+    add((void**)&w.qlo, 4 * d * ns);
+    add((void**)&w.qhi, 4 * d * ns);
+    add((void**)&w.orig, 4 * ns);
+    add((void**)&w.orig_tmp, 4 * ns);
+    add((void**)&w.perm, 4 * ns);
+    add((void**)&w.perm_tmp, 4 * ns);
+    add((void**)&w.cell_of, 4 * ns);
+    add((void**)&w.cell_start, 4 * (ns + 1));
+    add((void**)&w.cell_dims, 4 * d * ns);
+    add((void**)&w.cell_outer, 4 * ns);
+    add((void**)&w.css, 4 * d * ns);
+    add((void**)&w.csm, 4 * d * ns);
+    add((void**)&w.cbmin, 4 * d * ns);
+    add((void**)&w.cbmax, 4 * d * ns);
+    add((void**)&w.outer_begin, 4 * ((size_t)g.n_outer + 1));
+    add((void**)&w.hist, 4 * 256 * (size_t)tiles);
+    add((void**)&w.digit_total, 4 * 256);
+    add((void**)&w.block_sums, 4 * (size_t)nb);
+    add((void**)&w.wpart, 8 * 4 * (size_t)d * 2 * nw);
+    add((void**)&w.st_delta, 4 * 3 * (size_t)st_cap);
+    add((void**)&w.st_off, 3 * (size_t)st_cap * odp);
+    add((void**)&w.table, 4 * 3 * (size_t)TW);
+    add((void**)&w.ctrl, 4 * 16);
+    add((void**)&w.stamps, 8 * 4 * ((size_t)max_iter + 2));
+    add((void**)&w.labels, 4 * ns);
+    add((void**)&w.iter_flags, 4 * ((size_t)max_iter + 2));
+    add((void**)&xin, 4 * (size_t)g.n * d);
+    for (auto& p : plan) off += align_up(p.second);
+    if (off > I.cap) {
+        destroy_graph(I);
+        if (I.base) EGG_CHECK(cudaFree(I.base));
+        I.base = nullptr;
+        I.cap = 0;
+        size_t want = off + off / 8;
+        EGG_CHECK(cudaMalloc(&I.base, want));
+        I.cap = want;
+    }
+    char* b = (char*)I.base;
+    for (auto& p : plan) {
+        *p.first = b;
+        b += align_up(p.second);
+    }
+    I.used = off;
+    w.st_cap = st_cap;
+    for (int k = 0; k < 3; k++) w.st_count[k] = (int)st[k].delta.size();
+
+    // stencils and tables (pageable copies are synchronous; sizes are small)
+    std::vector<int> hd(3 * (size_t)st_cap, 0);
+    std::vector<signed char> ho(3 * (size_t)st_cap * odp, 0);
+    for (int k = 0; k < 3; k++) {
+        std::copy(st[k].delta.begin(), st[k].delta.end(), hd.begin() + (size_t)k * st_cap);
+        std::copy(st[k].off.begin(), st[k].off.end(), ho.begin() + (size_t)k * st_cap * odp);
+    }
+    std::vector<float> tab(3 * (size_t)TW);
+    for (int k = -g.table_k; k <= g.table_k; k++) {
+        const double a = (double)k * (double)g.side;
+        const double sh = sin(0.5 * a);
+        tab[k + g.table_k] = (float)sin(a);
+        tab[TW + k + g.table_k] = (float)cos(a);
+        tab[2 * TW + k + g.table_k] = (float)(2.0 * sh * sh);
+    }
+    EGG_CHECK(cudaMemcpyAsync(w.st_delta, hd.data(), hd.size() * 4, cudaMemcpyHostToDevice, I.st));
+    EGG_CHECK(cudaMemcpyAsync(w.st_off, ho.data(), ho.size(), cudaMemcpyHostToDevice, I.st));
+    EGG_CHECK(cudaMemcpyAsync(w.table, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice, I.st));
+    EGG_CHECK(cudaStreamSynchronize(I.st));
+
+    if ((int)((max_iter + 2) * 4) > I.h_stamps_cap) {
+        if (I.h_stamps) cudaFreeHost(I.h_stamps);
+        I.h_stamps_cap = (max_iter + 2) * 4;
+        EGG_CHECK(cudaMallocHost((void**)&I.h_stamps, 8 * (size_t)I.h_stamps_cap));
+    }
+    I.g = g;
+    I.w = w;
+    I.plan = make_plan(g);
+    I.xin = xin;
+    I.max_iter = max_iter;
+}
+
+// ------------------------------------------------------------------------
+// loop control kernels
+// ------------------------------------------------------------------------
+__global__ void k_ctrl_reset(Work w, int max_iter) {
+    if (threadIdx.x < 16) w.ctrl[threadIdx.x] = 0;
+    if (threadIdx.x == 0) w.ctrl[kCtrlMaxIter] = max_iter;
+}
+
+__global__ void k_iter_begin(Work w) {
+    const int it = w.ctrl[kCtrlIter];
+    w.ctrl[kCtrlFlag] = 1;
+    w.stamps[4 * it + 0] = globaltimer();
+}
+
+__global__ void k_iter_end(Work w, cudaGraphConditionalHandle h, int in_graph) {
+    const int it = w.ctrl[kCtrlIter];
+    const int flag = w.ctrl[kCtrlFlag];
+    w.iter_flags[it] = flag;
+    w.stamps[4 * it + 3] = globaltimer();
+    const int next = it + 1;
+    w.ctrl[kCtrlIter] = next;
+    const int done = flag != 0 || next >= w.ctrl[kCtrlMaxIter];
+    w.ctrl[kCtrlDone] = done;
+    if (in_graph && done) cudaGraphSetConditional(h, 0);
+}
+
+// whether the extra check ran in iteration `it` is visible as stamps[2] < stamps[3]
+// of that iteration; extra_checks counts flags that reached the extra check
+__global__ void k_mark_extra(Work w) {
+    if (w.ctrl[kCtrlFlag] != 0) atomicAdd(w.ctrl + kCtrlExtraRuns, 1);
+}
+
+// One iteration of the loop body.  With prof (8 events), the four kernel
+// groups are bracketed by CUDA events on the launching stream.
+void enqueue_iteration(Instance& I, cudaGraphConditionalHandle h, int in_graph, cudaEvent_t* prof = nullptr) {
+    cudaStream_t st = I.st;
+    auto mark = [&](int k) {
+        if (prof) EGG_CHECK(cudaEventRecord(prof[k], st));
+    };
+    k_iter_begin<<<1, 1, 0, st>>>(I.w);
+    mark(0);
+    launch_build(I.g, I.w, I.plan, st);
+    mark(1);
+    mark(2);
+    launch_cell_sums(I.g, I.w, st);
+    mark(3);
+    mark(4);
+    launch_update(I.g, I.w, nullptr, st);
+    mark(5);
+    k_mark_extra<<<1, 1, 0, st>>>(I.w);
+    mark(6);
+    launch_extra_check(I.g, I.w, st);
+    mark(7);
+    k_iter_end<<<1, 1, 0, st>>>(I.w, h, in_graph);
+}
+
+std::vector<char> graph_key(const Instance& I) {
+    std::vector<char> k(sizeof(Geom) + sizeof(Work) + sizeof(int));
+    memcpy(k.data(), &I.g, sizeof(Geom));
+    memcpy(k.data() + sizeof(Geom), &I.w, sizeof(Work));
+    memcpy(k.data() + sizeof(Geom) + sizeof(Work), &I.max_iter, sizeof(int));
+    return k;
+}
+
+bool ensure_graph(Instance& I) {
+    auto key = graph_key(I);
+    if (I.exec && key == I.graph_key) return true;
+    destroy_graph(I);
+    cudaGraph_t graph = nullptr;
+    cudaGraphConditionalHandle h;
+    cudaError_t e = cudaGraphCreate(&graph, 0);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault);
+    cudaGraph_t body = nullptr;
+    if (e == cudaSuccess) {
+        cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
+        p.conditional.handle = h;
+        p.conditional.type = cudaGraphCondTypeWhile;
+        p.conditional.size = 1;
+        cudaGraphNode_t node;
+        e = cudaGraphAddNode(&node, graph, nullptr, 0, &p);
+        if (e == cudaSuccess) body = p.conditional.phGraph_out[0];
+    }
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(I.st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        enqueue_iteration(I, h, 1);
+        cudaGraph_t captured = nullptr;
+        e = cudaStreamEndCapture(I.st, &captured);
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&I.exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        I.exec = nullptr;
+        I.graph_failed = true;
+        return false;
+    }
+    I.graph_key = key;
+    return true;
+}
+
+bool is_device_ptr(const void* p) {
+    cudaPointerAttributes a;
+    cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// load x (host or device, row-major n x d) into Xn and reset the control words
+void load_input(Instance& I, const float* x) {
+    const Geom& g = I.g;
+    const float* src = x;
+    if (!is_device_ptr(x)) {
+        EGG_CHECK(cudaMemcpyAsync(I.xin, x, sizeof(float) * (size_t)g.n * g.d, cudaMemcpyHostToDevice, I.st));
+        src = I.xin;
+    }
+    k_ctrl_reset<<<1, 32, 0, I.st>>>(I.w, I.max_iter);
+    launch_transpose_in(g, I.w, src, I.st);
+}
+
+void check_status_bits(Instance& I) {
+    EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, 16 * sizeof(int), cudaMemcpyDeviceToHost, I.st));
+    EGG_CHECK(cudaStreamSynchronize(I.st));
+    if (I.h_ctrl[kCtrlStatus] & kErrNonFinite) throw ArgError{EGG_ERR_INPUT, "input holds NaN or Inf"};
+}
+
+void order_after(Instance& I, void* stream) {
+    // the internal stream waits for work the caller queued on `stream`
+    cudaStream_t cs = (cudaStream_t)stream;
+    EGG_CHECK(cudaEventRecord(I.ev[5], cs));
+    EGG_CHECK(cudaStreamWaitEvent(I.st, I.ev[5], 0));
+}
+
+int fail(int status, const std::string& msg) {
+    g_last_error = msg;
+    return status;
+}
+
+template <typename F>
+int guarded(F&& fn) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    g_last_error.clear();
+    try {
+        return fn();
+    } catch (const ArgError& e) {
+        return fail(e.status, e.msg);
+    } catch (const CudaError& e) {
+        cudaGetLastError();
+        return fail(e.code == cudaErrorNoDevice || e.code == cudaErrorInsufficientDriver ? EGG_ERR_NO_DEVICE
+                                                                                          : EGG_ERR_CUDA,
+                    std::string(cudaGetErrorString(e.code)) + " in " + e.where);
+    } catch (const std::bad_alloc&) {
+        return fail(EGG_ERR_INTERNAL, "host allocation failed");
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------
+// entry points
+// ------------------------------------------------------------------------
+int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_opts* opts_in, int32_t* labels,
+        egg_stats* stats, void* stream) {
+    if (!x || !labels) throw ArgError{EGG_ERR_ARG, "x and labels must not be NULL"};
+    egg_opts opts;
+    memset(&opts, 0, sizeof(opts));
+    if (opts_in) opts = *opts_in;
+    int max_iter = opts.max_iter > 0 ? opts.max_iter : 1000;
+    if (max_iter > 1000000) throw ArgError{EGG_ERR_ARG, "max_iter too large"};
+    if (opts.stop_rule != 0) throw ArgError{EGG_ERR_ARG, "stop_rule 1 (order parameter) is not available in this build"};
+    (void)lam;
+    Geom g = make_geom(n, d, eps);
+    Instance& I = instance();
+    EGG_CHECK(cudaEventRecord(I.ev[0], I.st));
+    order_after(I, stream);
+    prepare(I, g, max_iter);
+    load_input(I, x);
+    check_status_bits(I);
+    EGG_CHECK(cudaEventRecord(I.ev[1], I.st));
+
+    float kms[4] = {0, 0, 0, 0};
+    int kl[4] = {0, 0, 0, 0};
+    bool use_graph = opts.loop == 0 && opts.profile == 0 && ensure_graph(I);
+    if (use_graph) {
+        EGG_CHECK(cudaGraphLaunch(I.exec, I.st));
+    } else {
+        cudaEvent_t* prof = opts.profile ? I.prof : nullptr;
+        if (prof && !I.prof[0])
+            for (auto& e : I.prof) EGG_CHECK(cudaEventCreate(&e));
+        for (;;) {
+            enqueue_iteration(I, 0, 0, prof);
+            EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, 16 * sizeof(int), cudaMemcpyDeviceToHost, I.st));
+            EGG_CHECK(cudaStreamSynchronize(I.st));
+            if (prof) {
+                for (int k = 0; k < 4; k++) {
+                    float t = 0;
+                    EGG_CHECK(cudaEventElapsedTime(&t, prof[2 * k], prof[2 * k + 1]));
+                    kms[k] += t;
+                    kl[k]++;
+                }
+            }
+            if (I.h_ctrl[kCtrlDone]) break;
+        }
+    }
+    EGG_CHECK(cudaEventRecord(I.ev[2], I.st));
+    // final grid and labels (EGG_SynC.cu:1503-1522)
+    launch_build(I.g, I.w, I.plan, I.st);
+    const bool dev_out = is_device_ptr(labels);
+    int* lab = dev_out ? labels : I.w.labels;
+    launch_labels(I.g, I.w, lab, I.st);
+    EGG_CHECK(cudaEventRecord(I.ev[3], I.st));
+    if (!dev_out) EGG_CHECK(cudaMemcpyAsync(labels, lab, sizeof(int) * (size_t)g.n, cudaMemcpyDeviceToHost, I.st));
+    EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, 16 * sizeof(int), cudaMemcpyDeviceToHost, I.st));
+    EGG_CHECK(cudaEventRecord(I.ev[4], I.st));
+    EGG_CHECK(cudaStreamSynchronize(I.st));
+    EGG_CHECK(cudaGetLastError());
+
+    const int iters = I.h_ctrl[kCtrlIter];
+    const int converged = I.h_ctrl[kCtrlFlag] != 0;
+    if (stats) {
+        const int M = I.h_ctrl[kCtrlM];
+        stats->iterations = iters;
+        stats->converged = converged;
+        stats->n_cells = M;
+        stats->extra_checks = I.h_ctrl[kCtrlExtraRuns];
+        stats->status_bits = I.h_ctrl[kCtrlStatus];
+        stats->workspace_bytes = (int64_t)I.used;
+        stats->order_param = -1.0;
+        stats->n_clusters = I.h_ctrl[kCtrlClusters];
+        EGG_CHECK(cudaMemcpy(I.h_stamps, I.w.stamps, 8 * 4 * (size_t)iters, cudaMemcpyDeviceToHost));
+        double st1 = 0, st2 = 0, st3 = 0;
+        for (int it = 0; it < iters; it++) {
+            const unsigned long long* s = I.h_stamps + 4 * it;
+            st1 += (double)(s[1] - s[0]);
+            st2 += (double)(s[2] - s[1]);
+            st3 += (double)(s[3] - s[2]);
+            if (stats->itr_ms && it < stats->itr_cap) stats->itr_ms[it] = (float)((s[3] - s[0]) * 1e-6);
+        }
+        float t01, t23, t34, t04;
+        EGG_CHECK(cudaEventElapsedTime(&t01, I.ev[0], I.ev[1]));
+        EGG_CHECK(cudaEventElapsedTime(&t23, I.ev[2], I.ev[3]));
+        EGG_CHECK(cudaEventElapsedTime(&t34, I.ev[3], I.ev[4]));
+        EGG_CHECK(cudaEventElapsedTime(&t04, I.ev[0], I.ev[4]));
+        stats->stage_ms[0] = t01;
+        stats->stage_ms[1] = (float)(st1 * 1e-6);
+        stats->stage_ms[2] = (float)(st2 * 1e-6);
+        stats->stage_ms[3] = (float)(st3 * 1e-6);
+        stats->stage_ms[4] = t23;
+        stats->stage_ms[5] = t34;
+        stats->total_ms = t04;
+        for (int k = 0; k < 4; k++) {
+            stats->kernel_ms[k] = kms[k];
+            stats->kernel_launches[k] = kl[k];
+        }
+        // launches: reset + transpose, per iteration (begin, build, 2 cell
+        // sums, update, mark, 2 extra, end), final build + labels
+        const int build_l = 3 * I.plan.count + 4;
+        stats->launches = 2 + iters * (build_l + 8) + build_l + 1;
+    }
+    if (I.h_ctrl[kCtrlStatus] & ~kErrNonFinite)
+        throw ArgError{EGG_ERR_INTERNAL, "kernel consistency check failed (status bits " +
+                                             std::to_string(I.h_ctrl[kCtrlStatus]) + ")"};
+    return converged ? EGG_OK : EGG_MAX_ITER;
+}
+
+int step(const float* x, int64_t n, int32_t d, float eps, float* x_next, int32_t* counts, int32_t* flags,
+         void* stream) {
+    if (!x || !x_next || !flags) throw ArgError{EGG_ERR_ARG, "x, x_next and flags must not be NULL"};
+    Geom g = make_geom(n, d, eps);
+    Instance& I = instance();
+    order_after(I, stream);
+    prepare(I, g, 4);
+    load_input(I, x);
+    check_status_bits(I);
+    cudaStream_t st = I.st;
+    k_iter_begin<<<1, 1, 0, st>>>(I.w);
+    launch_build(I.g, I.w, I.plan, st);
+    launch_cell_sums(I.g, I.w, st);
+    int* cnt_sorted = I.w.orig_tmp;  // free once the grid is built
+    launch_update(I.g, I.w, cnt_sorted, st);
+    EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, 16 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    EGG_CHECK(cudaStreamSynchronize(st));
+    flags[0] = I.h_ctrl[kCtrlFlag];
+    launch_extra_check(I.g, I.w, st);
+    EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, 16 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    // updated positions back to the original order (staged in qlo, free now)
+    const bool dev_x = is_device_ptr(x_next);
+    float* xo = dev_x ? x_next : I.xin;
+    launch_unsort_positions(I.g, I.w, I.w.Xn, xo, st);
+    if (!dev_x) EGG_CHECK(cudaMemcpyAsync(x_next, xo, sizeof(float) * (size_t)g.n * g.d, cudaMemcpyDeviceToHost, st));
+    if (counts) {
+        const bool dev_c = is_device_ptr(counts);
+        int* co = dev_c ? counts : I.w.labels;
+        launch_unsort_int(I.g, I.w, cnt_sorted, co, st);
+        if (!dev_c) EGG_CHECK(cudaMemcpyAsync(counts, co, sizeof(int) * (size_t)g.n, cudaMemcpyDeviceToHost, st));
+    }
+    EGG_CHECK(cudaStreamSynchronize(st));
+    EGG_CHECK(cudaGetLastError());
+    flags[1] = I.h_ctrl[kCtrlFlag];
+    if (I.h_ctrl[kCtrlStatus] & ~kErrNonFinite)
+        throw ArgError{EGG_ERR_INTERNAL, "kernel consistency check failed"};
+    return EGG_OK;
+}
+
+int grid(const float* x, int64_t n, int32_t d, float eps, int32_t* order, int32_t* cell_of, int32_t* cell_start,
+         int32_t* n_cells, void* stream) {
+    if (!x || !order || !cell_of || !cell_start || !n_cells) throw ArgError{EGG_ERR_ARG, "NULL argument"};
+    Geom g = make_geom(n, d, eps);
+    Instance& I = instance();
+    order_after(I, stream);
+    prepare(I, g, 4);
+    load_input(I, x);
+    check_status_bits(I);
+    launch_build(I.g, I.w, I.plan, I.st);
+    EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, 16 * sizeof(int), cudaMemcpyDeviceToHost, I.st));
+    EGG_CHECK(cudaStreamSynchronize(I.st));
+    const int M = I.h_ctrl[kCtrlM];
+    auto out = [&](int32_t* dst, const int* src, size_t cnt) {
+        EGG_CHECK(cudaMemcpyAsync(dst, src, sizeof(int) * cnt, cudaMemcpyDefault, I.st));
+    };
+    out(order, I.w.orig, (size_t)g.n);
+    out(cell_of, I.w.cell_of, (size_t)g.n);
+    out(cell_start, I.w.cell_start, (size_t)M + 1);
+    EGG_CHECK(cudaStreamSynchronize(I.st));
+    EGG_CHECK(cudaGetLastError());
+    *n_cells = M;
+    return EGG_OK;
+}
+
+int release() {
+    for (auto& kv : g_inst) {
+        Instance* I = kv.second;
+        int cur = 0;
+        cudaGetDevice(&cur);
+        cudaSetDevice(I->dev);
+        destroy_graph(*I);
+        if (I->base) cudaFree(I->base);
+        if (I->h_ctrl) cudaFreeHost(I->h_ctrl);
+        if (I->h_stamps) cudaFreeHost(I->h_stamps);
+        for (auto e : I->ev)
+            if (e) cudaEventDestroy(e);
+        for (auto e : I->prof)
+            if (e) cudaEventDestroy(e);
+        if (I->st) cudaStreamDestroy(I->st);
+        cudaSetDevice(cur);
+        delete I;
+    }
+    g_inst.clear();
+    return EGG_OK;
+}
+
+}  // namespace egg
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+__attribute__((visibility("default"))) void egg_opts_default(egg_opts* opts) {
+    if (opts) memset(opts, 0, sizeof(*opts));
+}
+
+__attribute__((visibility("default"))) int egg_sync_run(const float* x, int64_t n, int32_t d, float eps, float lam,
+                                                        const egg_opts* opts, int32_t* labels, egg_stats* stats,
+                                                        void* stream) {
+    return egg::guarded([&] { return egg::run(x, n, d, eps, lam, opts, labels, stats, stream); });
+}
+
+__attribute__((visibility("default"))) int egg_sync_step(const float* x, int64_t n, int32_t d, float eps,
+                                                         float* x_next, int32_t* counts, int32_t* flags,
+                                                         void* stream) {
+    return egg::guarded([&] { return egg::step(x, n, d, eps, x_next, counts, flags, stream); });
+}
+
+__attribute__((visibility("default"))) int egg_sync_grid(const float* x, int64_t n, int32_t d, float eps,
+                                                         int32_t* order, int32_t* cell_of, int32_t* cell_start,
+                                                         int32_t* n_cells, void* stream) {
+    return egg::guarded([&] { return egg::grid(x, n, d, eps, order, cell_of, cell_start, n_cells, stream); });
+}
+
+__attribute__((visibility("default"))) const char* egg_status_str(int s) {
+    switch (s) {
+        case EGG_OK: return "EGG_OK";
+        case EGG_MAX_ITER: return "EGG_MAX_ITER";
+        case EGG_ERR_ARG: return "EGG_ERR_ARG";
+        case EGG_ERR_GEOMETRY: return "EGG_ERR_GEOMETRY";
+        case EGG_ERR_INPUT: return "EGG_ERR_INPUT";
+        case EGG_ERR_CUDA: return "EGG_ERR_CUDA";
+        case EGG_ERR_NO_DEVICE: return "EGG_ERR_NO_DEVICE";
+        case EGG_ERR_INTERNAL: return "EGG_ERR_INTERNAL";
+        default: return "EGG_UNKNOWN_STATUS";
+    }
+}
+
+__attribute__((visibility("default"))) const char* egg_last_error(void) { return egg::g_last_error.c_str(); }
+
+__attribute__((visibility("default"))) int egg_release(void) {
+    return egg::guarded([&] { return egg::release(); });
+}
+
+__attribute__((visibility("default"))) int egg_abi_version(void) { return EGG_SYNC_ABI_VERSION; }
+
+}  // extern "C"

@@ -1,0 +1,94 @@
+"""ctypes binding of libeggsync.so (the C ABI declared in include/eggsync.h).
+
+There is no fallback: if the shared library is missing or fails to load,
+importing this module raises, so no caller can silently run anything but the
+CUDA path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_PATH = Path(os.environ.get("EGGSYNC_LIB", Path(__file__).resolve().parent.parent / "lib" / "libeggsync.so"))
+
+EGG_OK = 0
+EGG_MAX_ITER = 1
+EGG_ERR_ARG = -1
+EGG_ERR_GEOMETRY = -2
+EGG_ERR_INPUT = -3
+EGG_ERR_CUDA = -4
+EGG_ERR_NO_DEVICE = -5
+EGG_ERR_INTERNAL = -6
+
+# every symbol include/eggsync.h declares
+EXPORTS = ("egg_opts_default", "egg_sync_run", "egg_sync_step", "egg_sync_grid", "egg_status_str",
+           "egg_last_error", "egg_release", "egg_abi_version")
+
+
+class EggOpts(C.Structure):
+    _fields_ = [("max_iter", C.c_int32), ("loop", C.c_int32), ("stop_rule", C.c_int32),
+                ("order_param", C.c_int32), ("profile", C.c_int32), ("reserved", C.c_int32 * 11)]
+
+
+class EggStats(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("n_cells", C.c_int32),
+                ("n_clusters", C.c_int32), ("extra_checks", C.c_int32), ("status_bits", C.c_int32),
+                ("workspace_bytes", C.c_int64), ("order_param", C.c_double), ("stage_ms", C.c_float * 6),
+                ("total_ms", C.c_float), ("itr_ms", C.POINTER(C.c_float)), ("itr_cap", C.c_int32),
+                ("kernel_ms", C.c_float * 4), ("kernel_launches", C.c_int32 * 4), ("launches", C.c_int32)]
+
+
+class EggError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s: %s" % (_status_name(status), msg))
+        self.status = status
+
+
+_lib = None
+
+
+def _status_name(s):
+    try:
+        return load().egg_status_str(int(s)).decode()
+    except Exception:
+        return str(s)
+
+
+def load():
+    """Load libeggsync.so once and declare the prototypes."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError("libeggsync.so not found at %s: build it with "
+                          "`python -c 'import __graft_entry__ as g; g.build()'`" % LIB_PATH)
+    L = C.CDLL(str(LIB_PATH))
+    vp = C.c_void_p
+    L.egg_opts_default.argtypes = [C.POINTER(EggOpts)]
+    L.egg_opts_default.restype = None
+    L.egg_sync_run.argtypes = [vp, C.c_int64, C.c_int32, C.c_float, C.c_float, C.POINTER(EggOpts), vp,
+                               C.POINTER(EggStats), vp]
+    L.egg_sync_run.restype = C.c_int
+    L.egg_sync_step.argtypes = [vp, C.c_int64, C.c_int32, C.c_float, vp, vp, vp, vp]
+    L.egg_sync_step.restype = C.c_int
+    L.egg_sync_grid.argtypes = [vp, C.c_int64, C.c_int32, C.c_float, vp, vp, vp, C.POINTER(C.c_int32), vp]
+    L.egg_sync_grid.restype = C.c_int
+    L.egg_status_str.argtypes = [C.c_int]
+    L.egg_status_str.restype = C.c_char_p
+    L.egg_last_error.argtypes = []
+    L.egg_last_error.restype = C.c_char_p
+    L.egg_release.argtypes = []
+    L.egg_release.restype = C.c_int
+    L.egg_abi_version.argtypes = []
+    L.egg_abi_version.restype = C.c_int
+    _lib = L
+    return L
+
+
+def check(status):
+    """Raise EggError for negative statuses; return the status otherwise."""
+    if status < 0:
+        msg = load().egg_last_error().decode(errors="replace")
+        raise EggError(status, msg)
+    return status

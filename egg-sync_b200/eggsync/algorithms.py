@@ -1,0 +1,188 @@
+"""Python front end of the B200 EGG-SynC (mirrors python/algorithms.py).
+
+The reference's front end JIT-builds a torch extension and exposes
+``EGG_SynC(D, eps) -> impl.EGG_SynC_wrapper(D, eps)``
+(python/algorithms.py:6-17, 110-111; boundary src/maps/map.cpp:31-33).
+Here ``impl`` is a thin object over the C ABI of libeggsync.so with the same
+method name, argument meaning and return value:
+
+    C, itr_times, stage_times, space = EGG_SynC(D, eps)
+
+* ``C``: float32 tensor (n,), the compacted final cell index of each point
+  whose final cell holds more than one point, else -1 (EGG_SynC.cu:1205-1227,
+  1527-1541);
+* ``itr_times``: float32 tensor (#iterations,), seconds per iteration;
+* ``stage_times``: float32 tensor (6,), seconds in the reference's stage slots
+  (allocating, build structure, update, extra check, clustering, copy-out);
+* ``space``: int32 tensor (1,), device workspace bytes.
+
+Unlike the reference, ``D`` may live on the host or on a CUDA device, its
+dtype must be float32 (checked; the reference only asserts it through
+``data_ptr<float>``), and failures raise ``EggError`` instead of exiting.
+``lam`` is accepted (the reference's EGG path ignores it, EGG_SynC.cu:1233).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Tuple
+
+import numpy as np
+
+from . import _lib
+from ._lib import EggError, EggOpts, EggStats, check
+
+DEFAULT_LAMBDA = 1 - 1e-3
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def _prepare(X):
+    """Return (pointer, n, d, keepalive, device_index or None, stream pointer)."""
+    if isinstance(X, np.ndarray):
+        if X.dtype != np.float32:
+            raise TypeError("EGG-SynC expects float32 data, got %s" % X.dtype)
+        A = np.ascontiguousarray(X)
+        if A.ndim != 2:
+            raise ValueError("D must be a 2-D n x d array")
+        return A.ctypes.data, A.shape[0], A.shape[1], A, None, None
+    torch = _torch()
+    if not isinstance(X, torch.Tensor):
+        raise TypeError("D must be a torch.Tensor or numpy.ndarray")
+    if X.dtype != torch.float32:
+        raise TypeError("EGG-SynC expects a float32 tensor, got %s" % X.dtype)
+    if X.dim() != 2:
+        raise ValueError("D must be a 2-D n x d tensor")
+    T = X.contiguous()
+    if T.is_cuda:
+        return T.data_ptr(), T.shape[0], T.shape[1], T, T.device.index, torch.cuda.current_stream(T.device).cuda_stream
+    return T.data_ptr(), T.shape[0], T.shape[1], T, None, None
+
+
+class _DeviceGuard:
+    def __init__(self, idx):
+        self.idx = idx
+        self.ctx = None
+
+    def __enter__(self):
+        if self.idx is not None:
+            self.ctx = _torch().cuda.device(self.idx)
+            self.ctx.__enter__()
+
+    def __exit__(self, *a):
+        if self.ctx is not None:
+            self.ctx.__exit__(*a)
+
+
+def egg_sync(D, eps: float, lam: float = DEFAULT_LAMBDA, max_iter: int = 0, loop: str = "graph",
+             labels_out=None, profile: bool = False) -> Tuple[object, dict]:
+    """Run EGG-SynC; return (int32 labels, stats dict).
+
+    ``labels_out`` may be a preallocated int32 numpy array or torch tensor
+    (host or device) of n entries; by default a host numpy array is returned.
+    ``loop`` is "graph" (device-resident loop) or "host".  ``profile`` times
+    every kernel group with CUDA events (host-driven loop)."""
+    L = _lib.load()
+    ptr, n, d, keep, dev, stream = _prepare(D)
+    if labels_out is None:
+        labels_out = np.empty(n, np.int32)
+    if isinstance(labels_out, np.ndarray):
+        if labels_out.dtype != np.int32 or labels_out.size != n or not labels_out.flags.c_contiguous:
+            raise ValueError("labels_out must be a contiguous int32 array of n entries")
+        lptr = labels_out.ctypes.data
+    else:
+        torch = _torch()
+        if labels_out.dtype != torch.int32 or labels_out.numel() != n or not labels_out.is_contiguous():
+            raise ValueError("labels_out must be a contiguous int32 tensor of n entries")
+        lptr = labels_out.data_ptr()
+    opts = EggOpts()
+    L.egg_opts_default(C.byref(opts))
+    opts.max_iter = int(max_iter)
+    opts.loop = {"graph": 0, "host": 1}[loop]
+    opts.profile = 1 if profile else 0
+    stats = EggStats()
+    cap = opts.max_iter if opts.max_iter > 0 else 1000
+    itr = (C.c_float * cap)()
+    stats.itr_ms = C.cast(itr, C.POINTER(C.c_float))
+    stats.itr_cap = cap
+    with _DeviceGuard(dev):
+        st = check(L.egg_sync_run(C.c_void_p(ptr), n, d, float(eps), float(lam), C.byref(opts), C.c_void_p(lptr),
+                                  C.byref(stats), C.c_void_p(stream) if stream else None))
+    del keep
+    info = {
+        "status": int(st),
+        "iterations": int(stats.iterations),
+        "converged": bool(stats.converged),
+        "n_cells": int(stats.n_cells),
+        "n_clusters": int(stats.n_clusters),
+        "extra_checks": int(stats.extra_checks),
+        "status_bits": int(stats.status_bits),
+        "workspace_bytes": int(stats.workspace_bytes),
+        "stage_ms": [float(v) for v in stats.stage_ms],
+        "total_ms": float(stats.total_ms),
+        "itr_ms": [float(itr[i]) for i in range(min(stats.iterations, cap))],
+        "kernel_ms": dict(zip(("build", "cell_sums", "update", "extra"), [float(v) for v in stats.kernel_ms])),
+        "kernel_launches": dict(zip(("build", "cell_sums", "update", "extra"),
+                                    [int(v) for v in stats.kernel_launches])),
+        "launches": int(stats.launches),
+    }
+    return labels_out, info
+
+
+def egg_step(D, eps: float):
+    """One iteration from D: (x_next float32 n x d, counts int32 n, flags (update, after extra check))."""
+    L = _lib.load()
+    ptr, n, d, keep, dev, stream = _prepare(D)
+    out = np.empty((n, d), np.float32)
+    cnt = np.empty(n, np.int32)
+    flags = np.zeros(2, np.int32)
+    with _DeviceGuard(dev):
+        check(L.egg_sync_step(C.c_void_p(ptr), n, d, float(eps), C.c_void_p(out.ctypes.data),
+                              C.c_void_p(cnt.ctypes.data), C.c_void_p(flags.ctypes.data),
+                              C.c_void_p(stream) if stream else None))
+    del keep
+    return out, cnt, (int(flags[0]), int(flags[1]))
+
+
+def egg_grid(D, eps: float):
+    """The double grid of D: (order, cell_of, cell_start) as int32 arrays."""
+    L = _lib.load()
+    ptr, n, d, keep, dev, stream = _prepare(D)
+    order = np.empty(n, np.int32)
+    cell_of = np.empty(n, np.int32)
+    start = np.empty(n + 1, np.int32)
+    M = C.c_int32(0)
+    with _DeviceGuard(dev):
+        check(L.egg_sync_grid(C.c_void_p(ptr), n, d, float(eps), C.c_void_p(order.ctypes.data),
+                              C.c_void_p(cell_of.ctypes.data), C.c_void_p(start.ctypes.data), C.byref(M),
+                              C.c_void_p(stream) if stream else None))
+    del keep
+    return order, cell_of, start[: M.value + 1].copy()
+
+
+class _Impl:
+    """Stand-in for the reference's JIT module object ``impl``."""
+
+    @staticmethod
+    def EGG_SynC_wrapper(D, eps, lam=DEFAULT_LAMBDA):
+        torch = _torch()
+        lab, info = egg_sync(D, eps, lam)
+        C_ = torch.from_numpy(lab.astype(np.float32))
+        itr_times = torch.tensor([t / 1000.0 for t in info["itr_ms"]], dtype=torch.float32)
+        stage_times = torch.tensor([t / 1000.0 for t in info["stage_ms"]], dtype=torch.float32)
+        space = torch.tensor([min(info["workspace_bytes"], 2**31 - 1)], dtype=torch.int32)
+        return [C_, itr_times, stage_times, space]
+
+
+impl = _Impl()
+
+
+def EGG_SynC(D, eps, lam=DEFAULT_LAMBDA):
+    """python/algorithms.py:110-111 ``EGG_SynC(D, eps)``, with the optional lambda."""
+    return impl.EGG_SynC_wrapper(D, eps, lam)
+
+
+__all__ = ["EGG_SynC", "impl", "egg_sync", "egg_step", "egg_grid", "EggError", "DEFAULT_LAMBDA"]

@@ -1,0 +1,115 @@
+/*
+ * eggsync.h -- C ABI of libeggsync.so, the B200 (sm_100a) implementation of
+ * the EGG-SynC synchronisation-clustering loop.
+ *
+ * Every entry point takes plain pointers and sizes.  Point arrays are n x d
+ * float32, row-major (point-major), values normalised to [0, 1] as the
+ * reference expects.  Input and output pointers may be host or device
+ * memory (detected per pointer).  Calls are synchronous: they return when
+ * the outputs are written.  Calls from several host threads are serialised
+ * inside the library.  No entry point exits the process; failures are
+ * returned as negative egg_status values with a message in egg_last_error().
+ */
+#ifndef EGGSYNC_H
+#define EGGSYNC_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EGG_SYNC_ABI_VERSION 1
+
+typedef enum egg_status {
+    EGG_OK = 0,
+    EGG_MAX_ITER = 1,        /* warning: stopped at opts->max_iter before convergence; labels are valid */
+    EGG_ERR_ARG = -1,        /* bad argument (null pointer, n < 1, d out of range, eps not positive) */
+    EGG_ERR_GEOMETRY = -2,   /* eps gives a grid the kernels do not support (width < 2 or > 65535) */
+    EGG_ERR_INPUT = -3,      /* input holds NaN or Inf */
+    EGG_ERR_CUDA = -4,       /* a CUDA call failed; see egg_last_error() */
+    EGG_ERR_NO_DEVICE = -5,  /* no CUDA device */
+    EGG_ERR_INTERNAL = -6    /* an internal consistency check failed */
+} egg_status;
+
+typedef struct egg_opts {
+    int32_t max_iter;     /* iteration cap; 0 = default (1000).  The reference has none. */
+    int32_t loop;         /* 0 = device-resident loop (one CUDA graph, conditional while node),
+                             1 = host-driven loop (one 4-byte readback per iteration) */
+    int32_t stop_rule;    /* 0 = the reference's convergence flag (EGG_SynC.cu:1322),
+                             1 = local order parameter >= lam (SynC.cpp:277-303 semantics) */
+    int32_t order_param;  /* 0 = off, 1 = report the final FP64 order parameter */
+    int32_t profile;      /* 1 = time every kernel group with CUDA events (host-driven loop) */
+    int32_t reserved[11];
+} egg_opts;
+
+typedef struct egg_stats {
+    int32_t iterations;    /* loop iterations run (the reference's #itr) */
+    int32_t converged;     /* 1 when the stop rule ended the loop */
+    int32_t n_cells;       /* non-empty inner cells of the final grid */
+    int32_t n_clusters;    /* final cells holding more than one point */
+    int32_t extra_checks;  /* iterations that ran the extra convergence check */
+    int32_t status_bits;   /* kernel-side warning bits (0 normally) */
+    int64_t workspace_bytes;
+    double order_param;    /* final local order parameter (FP64) when requested, else -1 */
+    float stage_ms[6];     /* the reference's stage slots (run_experiment.py:20): allocating,
+                              build structure, update, extra check, clustering, copy-out */
+    float total_ms;
+    float *itr_ms;         /* optional caller array of itr_cap entries: device time per iteration */
+    int32_t itr_cap;
+    float kernel_ms[4];    /* with opts->profile: summed CUDA-event time of the grid build, cell
+                              sums, update and extra-check kernel groups */
+    int32_t kernel_launches[4];  /* launches of each group's main kernel */
+    int32_t launches;      /* kernels the call launched (all groups, loop control included) */
+} egg_stats;
+
+/* Fill *opts with the defaults (all zero). */
+void egg_opts_default(egg_opts *opts);
+
+/* Cluster n points of dimension d with radius eps.
+ * Replaces EGG_SynC(float *h_D, int n, int d, float eps)
+ * (src/algorithms/EGG_SynC.cuh:11, EGG_SynC.cu:1229-1601), reached from
+ * EGG_SynC_wrapper(at::Tensor &D, float eps) (src/maps/map.cpp:31-33).
+ * lam is the order-parameter threshold; it is only used with
+ * opts->stop_rule == 1 (the reference ignores it, EGG_SynC.cu:1233).
+ * labels[n] receives the compacted final cell index of every point whose
+ * final cell holds more than one point, else -1 (EGG_SynC.cu:1205-1227).
+ * opts and stats may be NULL.  stream: a cudaStream_t the call orders
+ * itself after (NULL = legacy default stream). */
+int egg_sync_run(const float *x, int64_t n, int32_t d, float eps, float lam, const egg_opts *opts,
+                 int32_t *labels, egg_stats *stats, void *stream);
+
+/* One iteration of the loop from the given positions (inspection and
+ * parity testing).  Mirrors one pass of the while body at
+ * src/algorithms/EGG_SynC.cu:1322-1495: x_next[n*d] receives the updated
+ * positions (original point order), counts[n] (may be NULL) |N_eps(p)|,
+ * flags[0] the update kernel's convergence flag (EGG_SynC.cu:706-709) and
+ * flags[1] the flag after the extra check (EGG_SynC.cu:1425-1489). */
+int egg_sync_step(const float *x, int64_t n, int32_t d, float eps, float *x_next, int32_t *counts,
+                  int32_t *flags, void *stream);
+
+/* The double grid built from x (inspection and parity testing).  Replaces
+ * build_the_grid (src/algorithms/EGG_SynC.cu:248-341): order[i] = original
+ * index of the i-th cell-sorted point, cell_of[i] = its cell, cell_start
+ * (n+1 entries) = first sorted position of each cell plus the end,
+ * *n_cells = number of non-empty cells. */
+int egg_sync_grid(const float *x, int64_t n, int32_t d, float eps, int32_t *order, int32_t *cell_of,
+                  int32_t *cell_start, int32_t *n_cells, void *stream);
+
+/* Human-readable name of a status value. */
+const char *egg_status_str(int status);
+
+/* Message of the last failure on the calling thread ("" if none). */
+const char *egg_last_error(void);
+
+/* Free the cached device workspaces and graphs of every device. */
+int egg_release(void);
+
+/* EGG_SYNC_ABI_VERSION of the loaded library. */
+int egg_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EGGSYNC_H */

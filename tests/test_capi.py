@@ -1,0 +1,89 @@
+"""CPU tests of the C ABI: the library loads, exports every declared entry
+point, its struct layouts match the header, and argument errors come back
+as status codes (these paths return before any CUDA call)."""
+import ctypes as C
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import REPO
+from eggsync import _lib
+
+HEADER = REPO / "include" / "eggsync.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(egg_[a-z_]+)\s*\(", text)))
+
+
+def test_exports_every_declared_symbol(eggsync_lib):
+    names = declared_functions()
+    assert set(names) == set(_lib.EXPORTS)
+    for n in names:
+        assert hasattr(eggsync_lib, n), n
+    out = subprocess.run(["nm", "-D", "--defined-only", str(_lib.LIB_PATH)], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\bT (egg_\w+)", out))
+    assert set(names) <= exported
+    # nothing but the declared C ABI is exported under the egg_ prefix
+    assert exported == set(names)
+
+
+def test_abi_version_and_status_names(eggsync_lib):
+    assert eggsync_lib.egg_abi_version() == 1
+    assert eggsync_lib.egg_status_str(0) == b"EGG_OK"
+    assert eggsync_lib.egg_status_str(-4) == b"EGG_ERR_CUDA"
+    assert eggsync_lib.egg_status_str(12345) == b"EGG_UNKNOWN_STATUS"
+
+
+def test_struct_layout_matches_header(tmp_path):
+    src = tmp_path / "sz.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "eggsync.h"\n'
+                   'int main(){printf("%zu %zu %zu %zu %zu\\n", sizeof(egg_opts), sizeof(egg_stats),'
+                   ' offsetof(egg_stats, stage_ms), offsetof(egg_stats, itr_ms), offsetof(egg_stats, itr_cap));}\n')
+    exe = tmp_path / "sz"
+    subprocess.run(["gcc", "-I", str(REPO / "include"), str(src), "-o", str(exe)], check=True)
+    vals = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
+    assert vals == [C.sizeof(_lib.EggOpts), C.sizeof(_lib.EggStats), _lib.EggStats.stage_ms.offset,
+                    _lib.EggStats.itr_ms.offset, _lib.EggStats.itr_cap.offset]
+
+
+def _run(L, x, n, d, eps, labels):
+    return L.egg_sync_run(x, n, d, eps, 0.999, None, labels, None, None)
+
+
+def test_argument_errors(eggsync_lib):
+    L = eggsync_lib
+    x = np.zeros((10, 2), np.float32)
+    lab = np.zeros(10, np.int32)
+    xp, lp = C.c_void_p(x.ctypes.data), C.c_void_p(lab.ctypes.data)
+    assert _run(L, None, 10, 2, 0.05, lp) == _lib.EGG_ERR_ARG
+    assert _run(L, xp, 10, 2, 0.05, None) == _lib.EGG_ERR_ARG
+    assert _run(L, xp, 0, 2, 0.05, lp) == _lib.EGG_ERR_ARG
+    assert _run(L, xp, 10, 0, 0.05, lp) == _lib.EGG_ERR_ARG
+    assert _run(L, xp, 10, 65, 0.05, lp) == _lib.EGG_ERR_ARG
+    assert _run(L, xp, 10, 2, 0.0, lp) == _lib.EGG_ERR_ARG
+    assert _run(L, xp, 10, 2, -1.0, lp) == _lib.EGG_ERR_ARG
+    assert _run(L, xp, 10, 2, float("nan"), lp) == _lib.EGG_ERR_ARG
+    assert b"eps" in L.egg_last_error()
+    # eps so large that a dimension has fewer than two cells
+    assert _run(L, xp, 10, 2, 5.0, lp) == _lib.EGG_ERR_GEOMETRY
+    # eps so small that a dimension has more than 65535 cells
+    assert _run(L, xp, 10, 2, 1e-6, lp) == _lib.EGG_ERR_GEOMETRY
+    flags = np.zeros(2, np.int32)
+    assert L.egg_sync_step(None, 10, 2, 0.05, xp, None, C.c_void_p(flags.ctypes.data), None) == _lib.EGG_ERR_ARG
+
+
+def test_python_front_end_rejects_bad_input(eggsync_lib):
+    from eggsync import egg_sync
+
+    with pytest.raises(TypeError):
+        egg_sync(np.zeros((10, 2), np.float64), 0.05)
+    with pytest.raises(ValueError):
+        egg_sync(np.zeros(10, np.float32), 0.05)
+    with pytest.raises(_lib.EggError) as e:
+        egg_sync(np.zeros((10, 2), np.float32), 5.0)
+    assert e.value.status == _lib.EGG_ERR_GEOMETRY
