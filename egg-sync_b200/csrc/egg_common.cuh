@@ -123,12 +123,14 @@ __device__ __forceinline__ bool on_border_dim(float x, float side) {
     return (id != idm) || (id != idp);
 }
 
-// reference box distance terms for one dimension, EGG_SynC.cu:613-630
+// reference box distance terms for one dimension, EGG_SynC.cu:613-630.  The
+// face offsets are one fused multiply-add each: the reference's
+// `dim_id * side` followed by `-= x` is contracted by nvcc, and only this
+// rounding reproduces the reference's own results for points lying exactly
+// on cell faces.
 __device__ __forceinline__ void box_terms(float x, int cd, float side, float& sm, float& lg) {
-    float left = __fmul_rn((float)cd, side);
-    float right = __fmul_rn((float)(cd + 1), side);
-    left = __fsub_rn(left, x);
-    right = __fsub_rn(right, x);
+    float left = __fmaf_rn((float)cd, side, -x);
+    float right = __fmaf_rn((float)(cd + 1), side, -x);
     left = __fmul_rn(left, left);
     right = __fmul_rn(right, right);
     if (left < right) {

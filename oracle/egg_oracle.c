@@ -32,8 +32,10 @@
  *   - cell id:        (int)(x / side), value == width -> width-1, then clamp
  *                     into [0, width-1] (the reference is undefined outside
  *                     [0,1]; inside it the clamp never fires)
- *   - box distance:   left = g*side - x, right = (g+1)*side - x, squared,
- *                     the smaller/larger added per dimension, no contraction
+ *   - box distance:   left = fmaf(g, side, -x), right = fmaf(g+1, side, -x),
+ *                     each squared (rounded), the smaller/larger added per
+ *                     dimension (the fused face offset is the convention the
+ *                     reference's own B200 run reproduces, see g_face_fma)
  *   - point distance: acc = fmaf(diff, diff, acc) over l = 0..d-1
  *   - "sqrt(v) <= e": v <= T(e), T(e) the largest float whose sqrtf is <= e
  *                     (sqrtf is correctly rounded and monotone, so the two
@@ -141,6 +143,17 @@ static int g_box_mode = 0;
 
 ORACLE_API void egg_oracle_set_box_mode(int exact) { g_box_mode = exact ? 1 : 0; }
 
+/* Rounding convention of the box-distance face offsets: 0 = product rounded,
+ * then the subtraction (g*side rounded, minus x); 1 = one fused multiply-add
+ * fmaf(g, side, -x).  The two differ only when x sits (almost) exactly on a
+ * cell face.  Only 1 reproduces the reference EGG-SynC run on a B200 for
+ * points placed exactly on cell faces (tests/golden/ref_egg_borders.npz:
+ * 20 iterations and the same partition; 0 gives 16 iterations), i.e. nvcc
+ * contracts the reference's `g * side` followed by `-= x` into one FMA. */
+static int g_face_fma = 1;
+
+ORACLE_API void egg_oracle_set_face_fma(int on) { g_face_fma = on ? 1 : 0; }
+
 /* reference box distance of point x to the cell with dim ids cd, EGG_SynC.cu:613-633.
  * In mode 1 the last cell of a dimension is also open-ended: the clamp
  * (value == width -> width-1, EGG_SynC.cu:69-71) puts points up to 1.0 in a
@@ -149,10 +162,16 @@ static inline void box_dist2(const float *x, const int *cd, int d, const egg_geo
     const float side = g->side;
     float s = 0.0f, L = 0.0f;
     for (int l = 0; l < d; l++) {
-        float left = (float)cd[l] * side;
-        float right = (float)(cd[l] + 1) * side;
-        left = left - x[l];
-        right = right - x[l];
+        float left, right;
+        if (g_face_fma) {
+            left = fmaf((float)cd[l], side, -x[l]);
+            right = fmaf((float)(cd[l] + 1), side, -x[l]);
+        } else {
+            left = (float)cd[l] * side;
+            right = (float)(cd[l] + 1) * side;
+            left = left - x[l];
+            right = right - x[l];
+        }
         const int last = cd[l] == g->width - 1;
         const int inside = (left <= 0.0f && (right >= 0.0f || last));
         left = left * left;

@@ -73,7 +73,13 @@ class Oracle:
                                              _i32p]
         L.egg_oracle_set_box_mode.argtypes = [C.c_int]
         L.egg_oracle_set_box_mode.restype = None
+        L.egg_oracle_set_face_fma.argtypes = [C.c_int]
+        L.egg_oracle_set_face_fma.restype = None
         self.L = L
+
+    def set_face_fma(self, on: bool):
+        """Rounding of the box-distance face offsets (see egg_oracle.c)."""
+        self.L.egg_oracle_set_face_fma(1 if on else 0)
 
     def set_box_mode(self, exact: bool):
         """False (default): the reference's cell test; True: the true minimum box distance."""
