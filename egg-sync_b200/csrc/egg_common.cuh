@@ -102,6 +102,9 @@ enum : int {
     kCtrlExtraRuns = 6,   // number of extra checks run
     kCtrlPairs = 7,       // annulus pairs examined in the last extra check
     kCtrlClusters = 8,    // final cells holding more than one point
+    kCtrlChanged = 9,     // some point left its cell since the last grid build
+    kCtrlGridValid = 10,  // the grid arrays describe the current sorted order
+    kCtrlBuilds = 11,     // grid builds actually performed (statistics)
 };
 
 // ------------------------------------------------------------------------
@@ -159,6 +162,26 @@ __device__ __forceinline__ float near_gap(float x, float lo, float hi) {
     if (x < lo) return __fsub_rn(lo, x);
     if (x > hi) return __fsub_rn(x, hi);
     return 0.0f;
+}
+
+// Squared distances from x to the nearest and to the farthest point of the
+// tight bounding box [lo, hi] of a cell's points, accumulated with the same
+// fused operation order as dist_step.  Every float step is monotone, so for
+// each point q of the cell near2 <= dist2(x, q) <= far2 holds exactly as the
+// kernels compute dist2: near2 > T proves no point passes "dist2 <= T", and
+// far2 <= T proves all of them do.
+__device__ __forceinline__ void tight_box_dist2(const float* x, const float* __restrict__ lo,
+                                                const float* __restrict__ hi, size_t stride, int d, float& near2,
+                                                float& far2) {
+    float a2 = 0.f, b2 = 0.f;
+    for (int l = 0; l < d; l++) {
+        const float L = __ldg(lo + (size_t)l * stride), H = __ldg(hi + (size_t)l * stride);
+        const float a = near_gap(x[l], L, H), b = far_gap(x[l], L, H);
+        a2 = __fmaf_rn(a, a, a2);
+        b2 = __fmaf_rn(b, b, b2);
+    }
+    near2 = a2;
+    far2 = b2;
 }
 
 __device__ __forceinline__ unsigned long long globaltimer() {

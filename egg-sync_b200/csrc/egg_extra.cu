@@ -120,12 +120,10 @@ __global__ void __launch_bounds__(128) k_ball_bbox(Geom g, Work w) {
         float sm2 = 0.f, lg2 = 0.f;
         for (int l = 0; l < d; l++) box_terms(xq[l], __ldg(w.cell_dims + (size_t)l * g.ns + c), g.side, sm2, lg2);
         if (!(sm2 <= g.t_half)) return true;
-        // all of the cell's points inside the eps/2 ball?
-        float far2 = 0.f;
-        for (int l = 0; l < d; l++) {
-            const float a = far_gap(xq[l], __ldg(w.cbmin + (size_t)l * g.ns + c), __ldg(w.cbmax + (size_t)l * g.ns + c));
-            far2 = __fmaf_rn(a, a, far2);
-        }
+        // none / all of the cell's points inside the eps/2 ball?
+        float near2, far2;
+        tight_box_dist2(xq, w.cbmin + c, w.cbmax + c, g.ns, d, near2, far2);
+        if (near2 > g.t_half) return true;
         if (far2 <= g.t_half) {
             for (int l = 0; l < d; l++) {
                 lo[l] = fminf(lo[l], __ldg(w.cbmin + (size_t)l * g.ns + c));
@@ -177,13 +175,8 @@ __global__ void __launch_bounds__(128) k_annulus(Geom g, Work w) {
         const bool included = sm2 <= g.t_extra;
         const bool fully = lg2 <= g.t_eps;
         if (!included || fully) return true;
-        float near2 = 0.f, far2 = 0.f;
-        for (int l = 0; l < d; l++) {
-            const float lo = __ldg(w.cbmin + (size_t)l * g.ns + c), hi = __ldg(w.cbmax + (size_t)l * g.ns + c);
-            const float a = near_gap(xp[l], lo, hi), b = far_gap(xp[l], lo, hi);
-            near2 = __fmaf_rn(a, a, near2);
-            far2 = __fmaf_rn(b, b, far2);
-        }
+        float near2, far2;
+        tight_box_dist2(xp, w.cbmin + c, w.cbmax + c, g.ns, d, near2, far2);
         if (near2 > g.t_extra || far2 <= g.t_eps) return true;
         const int qb = __ldg(w.cell_start + c), qe = __ldg(w.cell_start + c + 1);
         for (int q = qb; q < qe; q++) {

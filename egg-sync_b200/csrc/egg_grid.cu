@@ -68,11 +68,41 @@ __device__ __forceinline__ int digit_of(const Geom& g, const float* __restrict__
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// has any point left its cell?  A stable sort of unchanged keys is the
+// identity, so when no point changed cell the previous grid (order, cells,
+// outer ranges) is exactly the grid a rebuild would produce and every build
+// kernel below returns at once.  Also copies the positions into X.
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(256) k_check_cells(Geom g, Work w) {
+    const int d = D > 0 ? D : g.d;
+    const bool valid = w.ctrl[kCtrlGridValid] != 0;
+    bool changed = false;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+        const int c = valid ? w.cell_of[i] : 0;
+        for (int l = 0; l < d; l++) {
+            const float x = w.Xn[(size_t)l * g.ns + i];
+            w.X[(size_t)l * g.ns + i] = x;
+            if (valid) changed |= cell_dim(x, g) != w.cell_dims[(size_t)l * g.ns + c];
+        }
+    }
+    if (!valid) changed = true;
+    if (__syncthreads_or(changed) && threadIdx.x == 0) w.ctrl[kCtrlChanged] = 1;
+}
+
+__global__ void k_build_begin(int* ctrl) { ctrl[kCtrlChanged] = 0; }
+
+#define EGG_SKIP_IF_UNCHANGED(ctrl) \
+    if ((ctrl)[kCtrlChanged] == 0) return;
+
+// ---------------------------------------------------------------------------
 // radix sort pass: tile histograms
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kSortThreads) k_radix_hist(Geom g, const float* __restrict__ Xs,
                                                              const int* __restrict__ pin, int first, int dim,
-                                                             int shift, int* __restrict__ hist, int tiles) {
+                                                             int shift, int* __restrict__ hist, int tiles,
+                                                             const int* __restrict__ ctrl) {
+    EGG_SKIP_IF_UNCHANGED(ctrl);
     __shared__ int h[256];
     for (int t = threadIdx.x; t < 256; t += blockDim.x) h[t] = 0;
     __syncthreads();
@@ -90,7 +120,9 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_hist(Geom g, const float
 }
 
 // per-digit exclusive scan over tiles (one block per digit)
-__global__ void __launch_bounds__(256) k_radix_scan(int* __restrict__ hist, int tiles, int* __restrict__ digit_total) {
+__global__ void __launch_bounds__(256) k_radix_scan(int* __restrict__ hist, int tiles, int* __restrict__ digit_total,
+                                                    const int* __restrict__ ctrl) {
+    EGG_SKIP_IF_UNCHANGED(ctrl);
     int* h = hist + (size_t)blockIdx.x * tiles;
     const int per = (tiles + blockDim.x - 1) / blockDim.x;
     const int b = threadIdx.x * per;
@@ -112,7 +144,8 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(Geom g, const fl
                                                                 const int* __restrict__ pin, int first, int dim,
                                                                 int shift, const int* __restrict__ hist,
                                                                 const int* __restrict__ digit_total, int tiles,
-                                                                int* __restrict__ pout) {
+                                                                int* __restrict__ pout, const int* __restrict__ ctrl) {
+    EGG_SKIP_IF_UNCHANGED(ctrl);
     constexpr int kWarps = kSortThreads / 32;
     __shared__ int base[256];
     __shared__ int run[256];
@@ -165,6 +198,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(Geom g, const fl
 // ---------------------------------------------------------------------------
 template <int D>
 __global__ void __launch_bounds__(kHeadsBlock) k_gather_heads(Geom g, Work w, int identity) {
+    EGG_SKIP_IF_UNCHANGED(w.ctrl);
     const int d = D > 0 ? D : g.d;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     int head = 0;
@@ -189,6 +223,7 @@ __global__ void __launch_bounds__(kHeadsBlock) k_gather_heads(Geom g, Work w, in
 
 // single-block exclusive scan of the per-block head counts; M = total
 __global__ void __launch_bounds__(1024) k_scan_block_sums(int* __restrict__ bs, int nb, int* __restrict__ ctrl) {
+    EGG_SKIP_IF_UNCHANGED(ctrl);
     const int per = (nb + blockDim.x - 1) / blockDim.x;
     const int b = threadIdx.x * per;
     const int e = min(b + per, nb);
@@ -201,11 +236,16 @@ __global__ void __launch_bounds__(1024) k_scan_block_sums(int* __restrict__ bs, 
         bs[k] = run;
         run += v;
     }
-    if (threadIdx.x == 0) ctrl[kCtrlM] = total;
+    if (threadIdx.x == 0) {
+        ctrl[kCtrlM] = total;
+        ctrl[kCtrlGridValid] = 1;
+        ctrl[kCtrlBuilds] += 1;
+    }
 }
 
 template <int D>
 __global__ void __launch_bounds__(kHeadsBlock) k_heads_finalize(Geom g, Work w) {
+    EGG_SKIP_IF_UNCHANGED(w.ctrl);
     const int d = D > 0 ? D : g.d;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     int head = 0;
@@ -236,6 +276,7 @@ __global__ void __launch_bounds__(kHeadsBlock) k_heads_finalize(Geom g, Work w) 
 
 // outer_begin[o] = first cell whose outer id >= o, o in [0, n_outer]
 __global__ void k_outer_ranges(Geom g, Work w) {
+    EGG_SKIP_IF_UNCHANGED(w.ctrl);
     const int M = w.ctrl[kCtrlM];
     for (int o = blockIdx.x * blockDim.x + threadIdx.x; o <= g.n_outer; o += gridDim.x * blockDim.x)
         w.outer_begin[o] = lower_bound_i(w.cell_outer, 0, M, o);
@@ -465,16 +506,23 @@ void launch_sort(const Geom& g, const Work& w, const SortPlan& plan, cudaStream_
     for (int p = 0; p < plan.count; p++) {
         const int first = (p == 0);
         int* pout = bufs[out];
-        k_radix_hist<<<tiles, kSortThreads, 0, st>>>(g, w.Xn, pin, first, plan.dim[p], plan.shift[p], w.hist, tiles);
-        k_radix_scan<<<256, 256, 0, st>>>(w.hist, tiles, w.digit_total);
+        k_radix_hist<<<tiles, kSortThreads, 0, st>>>(g, w.Xn, pin, first, plan.dim[p], plan.shift[p], w.hist, tiles,
+                                                     w.ctrl);
+        k_radix_scan<<<256, 256, 0, st>>>(w.hist, tiles, w.digit_total, w.ctrl);
         k_radix_scatter<<<tiles, kSortThreads, 0, st>>>(g, w.Xn, pin, first, plan.dim[p], plan.shift[p], w.hist,
-                                                        w.digit_total, tiles, pout);
+                                                        w.digit_total, tiles, pout, w.ctrl);
         pin = pout;
         out ^= 1;
     }
 }
 
 void launch_build(const Geom& g, const Work& w, const SortPlan& plan, cudaStream_t st) {
+    {
+        k_build_begin<<<1, 1, 0, st>>>(w.ctrl);
+        int blocks = (g.n + 255) / 256;
+        if (blocks > 148 * 8) blocks = 148 * 8;
+        EGG_DISPATCH_D(g.d, k_check_cells, <<<blocks, 256, 0, st>>>(g, w));
+    }
     const int identity = plan.count == 0;
     if (!identity) launch_sort(g, w, plan, st);
     const int nb = (g.n + kHeadsBlock - 1) / kHeadsBlock;

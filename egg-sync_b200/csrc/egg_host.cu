@@ -568,7 +568,7 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
         }
         // launches: reset + transpose, per iteration (begin, build, 2 cell
         // sums, update, mark, 2 extra, end), final build + labels
-        const int build_l = 3 * I.plan.count + 4;
+        const int build_l = 3 * I.plan.count + 6;
         stats->launches = 2 + iters * (build_l + 8) + build_l + 1;
     }
     if (I.h_ctrl[kCtrlStatus] & ~kErrNonFinite)

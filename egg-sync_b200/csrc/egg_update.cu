@@ -56,6 +56,13 @@ __device__ int half_count(const Geom& g, const Work& w, const float* x, const in
             for (int l = 0; l < d; l++) box_terms(x[l], __ldg(w.cell_dims + (size_t)l * g.ns + c), g.side, sm2, lg2);
             if (!(lg2 <= g.t_eps)) continue;
             const int qb = __ldg(w.cell_start + c), qe = __ldg(w.cell_start + c + 1);
+            float near2, far2;
+            tight_box_dist2(x, w.cbmin + c, w.cbmax + c, g.ns, d, near2, far2);
+            if (near2 > g.t_half) continue;
+            if (far2 <= g.t_half) {
+                half += qe - qb;
+                continue;
+            }
             for (int q = qb; q < qe; q++) {
                 float d2 = 0.f;
                 for (int l = 0; l < d; l++) d2 = dist_step(__ldg(w.X + (size_t)l * g.ns + q), x[l], d2);
@@ -146,7 +153,27 @@ __global__ void __launch_bounds__(128) k_update(Geom g, Work w, int* __restrict_
                 }
                 N += qe - qb;
             } else {
-                // boundary cell: point by point
+                // boundary cell.  The tight box of its points decides it
+                // wholesale when all or none of them are within eps (the
+                // usual case once clusters have collapsed); otherwise walk.
+                float near2, far2;
+                tight_box_dist2(x, w.cbmin + c, w.cbmax + c, g.ns, d, near2, far2);
+                if (near2 > g.t_eps) continue;
+                if (far2 <= g.t_eps) {
+                    const float m = (float)(qe - qb);
+                    for (int l = 0; l < d; l++) {
+                        int k = kk[l] + K;
+                        if ((unsigned)k >= (unsigned)TW) { tab_err = true; k = K; }
+                        const float ss = __ldg(w.css + (size_t)l * g.ns + c);
+                        const float sm = __ldg(w.csm + (size_t)l * g.ns + c);
+                        const float ts = Ts[k], tc = Tc[k], tm = Tm[k];
+                        S[l] += ts * (m - sm) + tc * ss;
+                        Cm[l] += m * tm + tc * sm + ts * ss;
+                    }
+                    N += qe - qb;
+                    partial_in += qe - qb;
+                    continue;
+                }
                 float as[DM], am[DM];
                 for (int l = 0; l < d; l++) { as[l] = 0.f; am[l] = 0.f; }
                 int cnt = 0;
