@@ -57,7 +57,27 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--cpu-sample", type=int, default=0, help="points in the CPU-baseline sample (0 = auto)")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="for ncu: one warm-up run and one run of the workload through the host-driven loop, "
+                         "no timing, no CPU baseline")
     return ap.parse_args()
+
+
+def profile_run(args):
+    """One warm-up run and one run (host-driven loop: plain kernel launches)."""
+    import torch
+
+    from eggsync import data, egg_sync
+
+    dev = torch.device("cuda", 0)
+    c = data.c5(args.seed, n=args.n)
+    Xd = torch.from_numpy(c["X"]).to(dev)
+    lab = torch.empty(len(c["X"]), dtype=torch.int32, device=dev)
+    for k in range(2):
+        _, info = egg_sync(Xd, c["eps"], labels_out=lab, loop="host")
+    torch.cuda.synchronize(dev)
+    print(json.dumps({"profile_run": True, "n": len(c["X"]), "iterations": info["iterations"],
+                      "launches_per_run": info["launches"]}))
 
 
 def dist_setup(args):
@@ -309,6 +329,9 @@ def run_reference(args, rank, world):
 
 def main():
     args = parse()
+    if args.profile_run:
+        profile_run(args)
+        return
     rank, local, world, pg = dist_setup(args)
     try:
         if args.impl == "reference":

@@ -76,6 +76,98 @@ __device__ int half_count(const Geom& g, const Work& w, const float* x, const in
 
 }  // namespace
 
+namespace {
+
+template <int D>
+struct Acc {
+    float S[D > 0 ? D : kMaxDims];
+    float Cm[D > 0 ? D : kMaxDims];
+    int N;
+    int partial_in;
+    bool tab_err;
+};
+
+// m counted points of a cell at offsets k (= cell dims - own dims) with
+// SS = sum sin(delta), SM = sum (1 - cos(delta)) into the own-cell frame.
+template <int D>
+__device__ __forceinline__ void add_counted(Acc<D>& a, int d, const int* kk, float m, const float* SS, const float* SM,
+                                            const float* Ts, const float* Tc, const float* Tm, int K, int TW) {
+    for (int l = 0; l < d; l++) {
+        int k = kk[l] + K;
+        if ((unsigned)k >= (unsigned)TW) { a.tab_err = true; k = K; }
+        const float ts = Ts[k], tc = Tc[k], tm = Tm[k];
+        a.S[l] += ts * (m - SM[l]) + tc * SS[l];
+        a.Cm[l] += m * tm + tc * SM[l] + ts * SS[l];
+    }
+}
+
+// One candidate cell for one point: the reference's box test
+// (EGG_SynC.cu:613-636), then the aggregate (fully covered, or all points
+// provably within eps), nothing (no point provably within eps), or a walk.
+template <int D>
+__device__ __forceinline__ void visit_cell(const Geom& g, const Work& w, int c, const float* x, const int* gi,
+                                           Acc<D>& a, const float* Ts, const float* Tc, const float* Tm, int K, int TW) {
+    constexpr int DM = D > 0 ? D : kMaxDims;
+    const int d = D > 0 ? D : g.d;
+    float sm2 = 0.f, lg2 = 0.f;
+    int kk[DM];
+    for (int l = 0; l < d; l++) {
+        const int cd = __ldg(w.cell_dims + (size_t)l * g.ns + c);
+        box_terms(x[l], cd, g.side, sm2, lg2);
+        kk[l] = cd - gi[l];
+    }
+    if (!(sm2 <= g.t_eps)) return;
+    const int qb = __ldg(w.cell_start + c), qe = __ldg(w.cell_start + c + 1);
+    bool all_in = lg2 <= g.t_eps;
+    const bool full = all_in;
+    if (!full) {
+        float near2, far2;
+        tight_box_dist2(x, w.cbmin + c, w.cbmax + c, g.ns, d, near2, far2);
+        if (near2 > g.t_eps) return;
+        all_in = far2 <= g.t_eps;
+    }
+    if (all_in) {
+        float SS[DM], SM[DM];
+        for (int l = 0; l < d; l++) {
+            SS[l] = __ldg(w.css + (size_t)l * g.ns + c);
+            SM[l] = __ldg(w.csm + (size_t)l * g.ns + c);
+        }
+        add_counted<D>(a, d, kk, (float)(qe - qb), SS, SM, Ts, Tc, Tm, K, TW);
+        a.N += qe - qb;
+        if (!full) a.partial_in += qe - qb;
+        return;
+    }
+    float as[DM], am[DM];
+    for (int l = 0; l < d; l++) { as[l] = 0.f; am[l] = 0.f; }
+    int cnt = 0;
+    for (int q = qb; q < qe; q++) {
+        float d2 = 0.f;
+        for (int l = 0; l < d; l++) d2 = dist_step(__ldg(w.X + (size_t)l * g.ns + q), x[l], d2);
+        if (d2 <= g.t_eps) {
+            for (int l = 0; l < d; l++) {
+                as[l] += __ldg(w.sd + (size_t)l * g.ns + q);
+                am[l] += __ldg(w.md + (size_t)l * g.ns + q);
+            }
+            cnt++;
+        }
+    }
+    if (cnt) {
+        add_counted<D>(a, d, kk, (float)cnt, as, am, Ts, Tc, Tm, K, TW);
+        a.N += cnt;
+        a.partial_in += cnt;
+    }
+}
+
+}  // namespace
+
+// One thread per cell-sorted point.  When the 32 points of a warp share one
+// outer cell (the common case: sorted points are grouped by outer cell), the
+// warp resolves the stencil's outer cells in parallel (lane = stencil entry)
+// and then visits every candidate cell with all lanes in lockstep, so cell
+// records are broadcast loads and the dependent-load chain of the stencil
+// walk is paid once per warp instead of once per point.  Otherwise each lane
+// walks the stencil on its own.  Both paths visit a superset of the cells
+// the reference visits and apply the reference's per-point box test to each.
 template <int D>
 __global__ void __launch_bounds__(128) k_update(Geom g, Work w, int* __restrict__ counts) {
     constexpr int DM = D > 0 ? D : kMaxDims;
@@ -89,146 +181,124 @@ __global__ void __launch_bounds__(128) k_update(Geom g, Work w, int* __restrict_
     }
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.n) return;
+    if ((i & ~31) >= g.n) return;  // whole warp beyond n
+    const int lane = threadIdx.x & 31;
+    const bool valid = i < g.n;
+    const int iv = valid ? i : g.n - 1;  // lanes past n shadow the last point; their results are dropped
     const float* Ts = s_tab;
     const float* Tc = s_tab + TW;
     const float* Tm = s_tab + 2 * TW;
 
-    float x[DM], S[DM], Cm[DM];
+    float x[DM];
     int gi[DM];
     bool border = false;
     int obase = 0;
+    Acc<D> a;
     for (int l = 0; l < d; l++) {
-        x[l] = w.X[(size_t)l * g.ns + i];
+        x[l] = w.X[(size_t)l * g.ns + iv];
         gi[l] = cell_dim(x[l], g);
         border |= on_border_dim(x[l], g.side);
-        S[l] = 0.f;
-        Cm[l] = 0.f;
+        a.S[l] = 0.f;
+        a.Cm[l] = 0.f;
         if (l < g.od) obase += gi[l] * g.wpow[l];
     }
-    int N = 0, partial_in = 0;
-    bool tab_err = false;
-    const int own = w.cell_of[i];
+    a.N = 0;
+    a.partial_in = 0;
+    a.tab_err = false;
+    const int own = w.cell_of[iv];
     const int own_cnt = w.cell_start[own + 1] - w.cell_start[own];
 
     const int nst = w.st_count[0];
-    for (int s = 0; s < nst; s++) {
-        bool inb = true;
-        for (int l = 0; l < g.od; l++) {
-            int v = gi[l] + __ldg(w.st_off + (size_t)s * g.od + l);
-            inb = inb && (unsigned)v < (unsigned)g.width;
-        }
-        if (!inb) continue;
-        const int o = obase + __ldg(w.st_delta + s);
-        int cb = __ldg(w.outer_begin + o), ce = __ldg(w.outer_begin + o + 1);
-        if (cb >= ce) continue;
+    const int ob0 = __shfl_sync(0xffffffffu, obase, 0);
+    if (__all_sync(0xffffffffu, obase == ob0)) {
+        int zlo = 0, zhi = 0;
         if (g.od < d) {
-            // cells beyond r+1 in dimension od fail the box test (their gap
-            // exceeds (r+1)*side > eps), so the search keeps the visiting set
-            const int* keys = w.cell_dims + (size_t)g.od * g.ns;
-            cb = lower_bound_i(keys, cb, ce, gi[g.od] - g.r - 1);
-            ce = lower_bound_i(keys, cb, ce, gi[g.od] + g.r + 2);
+            zlo = zhi = gi[g.od];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                zlo = min(zlo, __shfl_xor_sync(0xffffffffu, zlo, o));
+                zhi = max(zhi, __shfl_xor_sync(0xffffffffu, zhi, o));
+            }
         }
-        for (int c = cb; c < ce; c++) {
-            float sm2 = 0.f, lg2 = 0.f;
-            int kk[DM];
-            for (int l = 0; l < d; l++) {
-                const int cd = __ldg(w.cell_dims + (size_t)l * g.ns + c);
-                box_terms(x[l], cd, g.side, sm2, lg2);
-                kk[l] = cd - gi[l];
-            }
-            if (!(sm2 <= g.t_eps)) continue;
-            const int qb = __ldg(w.cell_start + c), qe = __ldg(w.cell_start + c + 1);
-            if (lg2 <= g.t_eps) {
-                // fully inside the eps-ball: aggregate
-                const float m = (float)(qe - qb);
-                for (int l = 0; l < d; l++) {
-                    int k = kk[l] + K;
-                    if ((unsigned)k >= (unsigned)TW) { tab_err = true; k = K; }
-                    const float ss = __ldg(w.css + (size_t)l * g.ns + c);
-                    const float sm = __ldg(w.csm + (size_t)l * g.ns + c);
-                    const float ts = Ts[k], tc = Tc[k], tm = Tm[k];
-                    S[l] += ts * (m - sm) + tc * ss;
-                    Cm[l] += m * tm + tc * sm + ts * ss;
+        for (int s0 = 0; s0 < nst; s0 += 32) {
+            const int s = s0 + lane;
+            int cb = 0, ce = 0;
+            if (s < nst) {
+                bool inb = true;
+                for (int l = 0; l < g.od; l++) {
+                    const int v = gi[l] + __ldg(w.st_off + (size_t)s * g.od + l);
+                    inb = inb && (unsigned)v < (unsigned)g.width;
                 }
-                N += qe - qb;
-            } else {
-                // boundary cell.  The tight box of its points decides it
-                // wholesale when all or none of them are within eps (the
-                // usual case once clusters have collapsed); otherwise walk.
-                float near2, far2;
-                tight_box_dist2(x, w.cbmin + c, w.cbmax + c, g.ns, d, near2, far2);
-                if (near2 > g.t_eps) continue;
-                if (far2 <= g.t_eps) {
-                    const float m = (float)(qe - qb);
-                    for (int l = 0; l < d; l++) {
-                        int k = kk[l] + K;
-                        if ((unsigned)k >= (unsigned)TW) { tab_err = true; k = K; }
-                        const float ss = __ldg(w.css + (size_t)l * g.ns + c);
-                        const float sm = __ldg(w.csm + (size_t)l * g.ns + c);
-                        const float ts = Ts[k], tc = Tc[k], tm = Tm[k];
-                        S[l] += ts * (m - sm) + tc * ss;
-                        Cm[l] += m * tm + tc * sm + ts * ss;
+                if (inb) {
+                    const int o = obase + __ldg(w.st_delta + s);
+                    cb = __ldg(w.outer_begin + o);
+                    ce = __ldg(w.outer_begin + o + 1);
+                    if (cb < ce && g.od < d) {
+                        // cells beyond r+1 in dimension od fail the box test
+                        // (their gap exceeds (r+1)*side > eps) for every lane
+                        const int* keys = w.cell_dims + (size_t)g.od * g.ns;
+                        cb = lower_bound_i(keys, cb, ce, zlo - g.r - 1);
+                        ce = lower_bound_i(keys, cb, ce, zhi + g.r + 2);
                     }
-                    N += qe - qb;
-                    partial_in += qe - qb;
-                    continue;
-                }
-                float as[DM], am[DM];
-                for (int l = 0; l < d; l++) { as[l] = 0.f; am[l] = 0.f; }
-                int cnt = 0;
-                for (int q = qb; q < qe; q++) {
-                    float d2 = 0.f;
-                    for (int l = 0; l < d; l++) d2 = dist_step(__ldg(w.X + (size_t)l * g.ns + q), x[l], d2);
-                    if (d2 <= g.t_eps) {
-                        for (int l = 0; l < d; l++) {
-                            as[l] += __ldg(w.sd + (size_t)l * g.ns + q);
-                            am[l] += __ldg(w.md + (size_t)l * g.ns + q);
-                        }
-                        cnt++;
-                    }
-                }
-                if (cnt) {
-                    const float m = (float)cnt;
-                    for (int l = 0; l < d; l++) {
-                        int k = kk[l] + K;
-                        if ((unsigned)k >= (unsigned)TW) { tab_err = true; k = K; }
-                        const float ts = Ts[k], tc = Tc[k], tm = Tm[k];
-                        S[l] += ts * (m - am[l]) + tc * as[l];
-                        Cm[l] += m * tm + tc * am[l] + ts * as[l];
-                    }
-                    N += cnt;
-                    partial_in += cnt;
                 }
             }
+            unsigned live = __ballot_sync(0xffffffffu, cb < ce);
+            while (live) {
+                const int src = __ffs(live) - 1;
+                live &= live - 1;
+                const int b = __shfl_sync(0xffffffffu, cb, src);
+                const int e = __shfl_sync(0xffffffffu, ce, src);
+                for (int c = b; c < e; c++) visit_cell<D>(g, w, c, x, gi, a, Ts, Tc, Tm, K, TW);
+            }
+        }
+    } else {
+        for (int s = 0; s < nst; s++) {
+            bool inb = true;
+            for (int l = 0; l < g.od; l++) {
+                const int v = gi[l] + __ldg(w.st_off + (size_t)s * g.od + l);
+                inb = inb && (unsigned)v < (unsigned)g.width;
+            }
+            if (!inb) continue;
+            const int o = obase + __ldg(w.st_delta + s);
+            int cb = __ldg(w.outer_begin + o), ce = __ldg(w.outer_begin + o + 1);
+            if (cb >= ce) continue;
+            if (g.od < d) {
+                const int* keys = w.cell_dims + (size_t)g.od * g.ns;
+                cb = lower_bound_i(keys, cb, ce, gi[g.od] - g.r - 1);
+                ce = lower_bound_i(keys, cb, ce, gi[g.od] + g.r + 2);
+            }
+            for (int c = cb; c < ce; c++) visit_cell<D>(g, w, c, x, gi, a, Ts, Tc, Tm, K, TW);
         }
     }
 
+    const int N = a.N;
     const float fN = (float)N;
-    for (int l = 0; l < d; l++) {
-        const float corner = __fmul_rn((float)gi[l], g.side);
-        const float phi = x[l] - corner;
-        float sp, cp;
-        sincosf(phi, &sp, &cp);
-        const float A = cp * S[l] - sp * (fN - Cm[l]);
-        w.Xn[(size_t)l * g.ns + i] = x[l] + A / fN;
+    if (valid) {
+        for (int l = 0; l < d; l++) {
+            const float corner = __fmul_rn((float)gi[l], g.side);
+            const float phi = x[l] - corner;
+            float sp, cp;
+            sincosf(phi, &sp, &cp);
+            const float A = cp * a.S[l] - sp * (fN - a.Cm[l]);
+            w.Xn[(size_t)l * g.ns + i] = x[l] + A / fN;
+        }
+        if (counts) counts[i] = N;
     }
-    if (counts) counts[i] = N;
 
     // convergence flag, EGG_SynC.cu:706-709.  half_count <= N - partial_in,
     // so a border point with neighbours in a partial cell always violates.
-    bool viol;
-    if (!border) viol = (N != own_cnt);
-    else if (partial_in > 0) viol = true;
-    else if (N == own_cnt) viol = false;
-    else viol = (N != half_count<D>(g, w, x, gi, obase, own, own_cnt));
-    const unsigned act = __activemask();
-    const unsigned vb = __ballot_sync(act, viol);
-    if (vb && (threadIdx.x & 31) == __ffs(act) - 1) {
+    bool viol = false;
+    if (valid) {
+        if (!border) viol = (N != own_cnt);
+        else if (a.partial_in > 0) viol = true;
+        else if (N == own_cnt) viol = false;
+        else viol = (N != half_count<D>(g, w, x, gi, obase, own, own_cnt));
+    }
+    if (__any_sync(0xffffffffu, viol) && lane == 0) {
         volatile int* f = w.ctrl + kCtrlFlag;
         if (*f != 0) *f = 0;
     }
-    if (tab_err) atomicOr(w.ctrl + kCtrlStatus, kErrTable);
+    if (a.tab_err) atomicOr(w.ctrl + kCtrlStatus, kErrTable);
 }
 
 #define EGG_DISPATCH_D(d, KERNEL, ...)                \
