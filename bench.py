@@ -45,7 +45,7 @@ WORKLOAD = "egg-sync plain loop, 1M x 3D, 50 Gaussian clusters + 10% noise, eps 
 L2_FLUSH_BYTES = 256 << 20
 # Iterations the reference EGG semantics take on this workload (measured by
 # the plain GPU path; used only to extrapolate the CPU baseline).
-C5_ITERATIONS = None
+C5_ITERATIONS = 191
 
 
 def parse():

@@ -90,6 +90,12 @@ struct Work {
     int* labels;       // [ns] output labels (original order)
     int* iter_flags;   // [max_iter] flag after each iteration
     int* iter_counts;  // reserved
+    // incremental update: outer cells touched by a moved point (old or new
+    // position) in the last update, ping-pong by iteration parity; the
+    // stencil dilation of those marks; the last violation bit of every point
+    unsigned char* dirty[2];   // [n_outer]
+    unsigned char* need;       // [n_outer]
+    unsigned char* viol_orig;  // [ns] by original index
 };
 
 enum : int {
@@ -105,6 +111,9 @@ enum : int {
     kCtrlChanged = 9,     // some point left its cell since the last grid build
     kCtrlGridValid = 10,  // the grid arrays describe the current sorted order
     kCtrlBuilds = 11,     // grid builds actually performed (statistics)
+    kCtrlForce = 12,      // recompute every point (first iteration of a run)
+    kCtrlComputed = 13,   // points recomputed by the update (statistics)
+    kCtrlFullUpdate = 14, // recompute every point in every iteration
 };
 
 // ------------------------------------------------------------------------

@@ -259,6 +259,10 @@ void prepare(Instance& I, const Geom& g, int max_iter) {
     add((void**)&w.labels, 4 * ns);
     add((void**)&w.iter_flags, 4 * ((size_t)max_iter + 2));
     add((void**)&xin, 4 * (size_t)g.n * d);
+    add((void**)&w.dirty[0], (size_t)g.n_outer + 1);
+    add((void**)&w.dirty[1], (size_t)g.n_outer + 1);
+    add((void**)&w.need, (size_t)g.n_outer + 1);
+    add((void**)&w.viol_orig, ns);
     for (auto& p : plan) off += align_up(p.second);
     if (off > I.cap) {
         destroy_graph(I);
@@ -313,9 +317,14 @@ void prepare(Instance& I, const Geom& g, int max_iter) {
 // ------------------------------------------------------------------------
 // loop control kernels
 // ------------------------------------------------------------------------
-__global__ void k_ctrl_reset(Work w, int max_iter) {
+__global__ void k_ctrl_reset(Work w, int max_iter, int full_update) {
     if (threadIdx.x < 16) w.ctrl[threadIdx.x] = 0;
-    if (threadIdx.x == 0) w.ctrl[kCtrlMaxIter] = max_iter;
+    __syncwarp();
+    if (threadIdx.x == 0) {
+        w.ctrl[kCtrlMaxIter] = max_iter;
+        w.ctrl[kCtrlForce] = 1;
+        w.ctrl[kCtrlFullUpdate] = full_update;
+    }
 }
 
 __global__ void k_iter_begin(Work w) {
@@ -331,6 +340,7 @@ __global__ void k_iter_end(Work w, cudaGraphConditionalHandle h, int in_graph) {
     w.stamps[4 * it + 3] = globaltimer();
     const int next = it + 1;
     w.ctrl[kCtrlIter] = next;
+    w.ctrl[kCtrlForce] = w.ctrl[kCtrlFullUpdate];
     const int done = flag != 0 || next >= w.ctrl[kCtrlMaxIter];
     w.ctrl[kCtrlDone] = done;
     if (in_graph && done) cudaGraphSetConditional(h, 0);
@@ -355,6 +365,7 @@ void enqueue_iteration(Instance& I, cudaGraphConditionalHandle h, int in_graph, 
     mark(1);
     mark(2);
     launch_cell_sums(I.g, I.w, st);
+    launch_need(I.g, I.w, st);
     mark(3);
     mark(4);
     launch_update(I.g, I.w, nullptr, st);
@@ -421,14 +432,14 @@ bool is_device_ptr(const void* p) {
 }
 
 // load x (host or device, row-major n x d) into Xn and reset the control words
-void load_input(Instance& I, const float* x) {
+void load_input(Instance& I, const float* x, int full_update = 0) {
     const Geom& g = I.g;
     const float* src = x;
     if (!is_device_ptr(x)) {
         EGG_CHECK(cudaMemcpyAsync(I.xin, x, sizeof(float) * (size_t)g.n * g.d, cudaMemcpyHostToDevice, I.st));
         src = I.xin;
     }
-    k_ctrl_reset<<<1, 32, 0, I.st>>>(I.w, I.max_iter);
+    k_ctrl_reset<<<1, 32, 0, I.st>>>(I.w, I.max_iter, full_update);
     launch_transpose_in(g, I.w, src, I.st);
 }
 
@@ -488,7 +499,7 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
     EGG_CHECK(cudaEventRecord(I.ev[0], I.st));
     order_after(I, stream);
     prepare(I, g, max_iter);
-    load_input(I, x);
+    load_input(I, x, opts.full_update ? 1 : 0);
     check_status_bits(I);
     EGG_CHECK(cudaEventRecord(I.ev[1], I.st));
 
@@ -522,6 +533,14 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
     const bool dev_out = is_device_ptr(labels);
     int* lab = dev_out ? labels : I.w.labels;
     launch_labels(I.g, I.w, lab, I.st);
+    if (opts.positions_out) {
+        const bool dev_p = is_device_ptr(opts.positions_out);
+        float* po = dev_p ? opts.positions_out : I.xin;
+        launch_unsort_positions(I.g, I.w, I.w.X, po, I.st);
+        if (!dev_p)
+            EGG_CHECK(cudaMemcpyAsync(opts.positions_out, po, sizeof(float) * (size_t)g.n * g.d,
+                                      cudaMemcpyDeviceToHost, I.st));
+    }
     EGG_CHECK(cudaEventRecord(I.ev[3], I.st));
     if (!dev_out) EGG_CHECK(cudaMemcpyAsync(labels, lab, sizeof(int) * (size_t)g.n, cudaMemcpyDeviceToHost, I.st));
     EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, 16 * sizeof(int), cudaMemcpyDeviceToHost, I.st));
@@ -569,7 +588,7 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
         // launches: reset + transpose, per iteration (begin, build, 2 cell
         // sums, update, mark, 2 extra, end), final build + labels
         const int build_l = 3 * I.plan.count + 6;
-        stats->launches = 2 + iters * (build_l + 8) + build_l + 1;
+        stats->launches = 2 + iters * (build_l + 9) + build_l + 1;
     }
     if (I.h_ctrl[kCtrlStatus] & ~kErrNonFinite)
         throw ArgError{EGG_ERR_INTERNAL, "kernel consistency check failed (status bits " +
@@ -590,6 +609,7 @@ int step(const float* x, int64_t n, int32_t d, float eps, float* x_next, int32_t
     k_iter_begin<<<1, 1, 0, st>>>(I.w);
     launch_build(I.g, I.w, I.plan, st);
     launch_cell_sums(I.g, I.w, st);
+    launch_need(I.g, I.w, st);
     int* cnt_sorted = I.w.orig_tmp;  // free once the grid is built
     launch_update(I.g, I.w, cnt_sorted, st);
     EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, 16 * sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -27,6 +27,8 @@ void launch_unsort_int(const Geom& g, const Work& w, const int* src, int* out, c
 // update + flag (egg_update.cu); counts (nullable) receives |N_eps(p)| per
 // sorted point
 void launch_update(const Geom& g, const Work& w, int* counts, cudaStream_t st);
+// stencil dilation of the outer cells touched by moved points (incremental update)
+void launch_need(const Geom& g, const Work& w, cudaStream_t st);
 
 // extra convergence check (egg_extra.cu)
 void launch_extra_check(const Geom& g, const Work& w, cudaStream_t st);

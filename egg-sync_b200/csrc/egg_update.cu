@@ -189,18 +189,44 @@ __global__ void __launch_bounds__(128) k_update(Geom g, Work w, int* __restrict_
     const float* Tc = s_tab + TW;
     const float* Tm = s_tab + 2 * TW;
 
+    const int it = w.ctrl[kCtrlIter];
     float x[DM];
     int gi[DM];
-    bool border = false;
     int obase = 0;
-    Acc<D> a;
     for (int l = 0; l < d; l++) {
         x[l] = w.X[(size_t)l * g.ns + iv];
         gi[l] = cell_dim(x[l], g);
+        if (l < g.od) obase += gi[l] * g.wpow[l];
+    }
+
+    // Incremental update: when no point of this warp has a moved point (old
+    // or new position) anywhere in its stencil region since the last update,
+    // every input of its update is unchanged, so the result is the same bit
+    // for bit: keep the position and the last violation bit.
+    const bool need_me = w.ctrl[kCtrlForce] != 0 || w.need[obase] != 0;
+    if (!__any_sync(0xffffffffu, need_me)) {
+        bool viol = false;
+        if (valid) {
+            for (int l = 0; l < d; l++) w.Xn[(size_t)l * g.ns + i] = x[l];
+            viol = w.viol_orig[w.orig[i]] != 0;
+        }
+        if (__any_sync(0xffffffffu, viol) && lane == 0) {
+            volatile int* f = w.ctrl + kCtrlFlag;
+            if (*f != 0) *f = 0;
+        }
+        return;
+    }
+    {
+        const unsigned vm = __ballot_sync(0xffffffffu, valid);
+        if (lane == 0) atomicAdd(w.ctrl + kCtrlComputed, __popc(vm));
+    }
+
+    bool border = false;
+    Acc<D> a;
+    for (int l = 0; l < d; l++) {
         border |= on_border_dim(x[l], g.side);
         a.S[l] = 0.f;
         a.Cm[l] = 0.f;
-        if (l < g.od) obase += gi[l] * g.wpow[l];
     }
     a.N = 0;
     a.partial_in = 0;
@@ -273,6 +299,8 @@ __global__ void __launch_bounds__(128) k_update(Geom g, Work w, int* __restrict_
 
     const int N = a.N;
     const float fN = (float)N;
+    bool moved = false;
+    int onew = 0;
     if (valid) {
         for (int l = 0; l < d; l++) {
             const float corner = __fmul_rn((float)gi[l], g.side);
@@ -280,7 +308,10 @@ __global__ void __launch_bounds__(128) k_update(Geom g, Work w, int* __restrict_
             float sp, cp;
             sincosf(phi, &sp, &cp);
             const float A = cp * a.S[l] - sp * (fN - a.Cm[l]);
-            w.Xn[(size_t)l * g.ns + i] = x[l] + A / fN;
+            const float xn = x[l] + A / fN;
+            w.Xn[(size_t)l * g.ns + i] = xn;
+            moved |= __float_as_uint(xn) != __float_as_uint(x[l]);
+            if (l < g.od) onew += cell_dim(xn, g) * g.wpow[l];
         }
         if (counts) counts[i] = N;
     }
@@ -293,6 +324,12 @@ __global__ void __launch_bounds__(128) k_update(Geom g, Work w, int* __restrict_
         else if (a.partial_in > 0) viol = true;
         else if (N == own_cnt) viol = false;
         else viol = (N != half_count<D>(g, w, x, gi, obase, own, own_cnt));
+        w.viol_orig[w.orig[i]] = viol ? 1 : 0;
+        if (moved) {
+            unsigned char* dcur = w.dirty[it & 1];
+            dcur[obase] = 1;
+            dcur[onew] = 1;
+        }
     }
     if (__any_sync(0xffffffffu, viol) && lane == 0) {
         volatile int* f = w.ctrl + kCtrlFlag;
@@ -313,6 +350,45 @@ __global__ void __launch_bounds__(128) k_update(Geom g, Work w, int* __restrict_
         case 16: KERNEL<16> __VA_ARGS__; break;       \
         default: KERNEL<0> __VA_ARGS__; break;        \
     }
+
+// need[o] = some outer cell of o's stencil holds a point that moved in the
+// last update (dirty of the previous iteration); also clears the dirty marks
+// the coming update will write.
+__global__ void k_need(Geom g, Work w) {
+    const int it = w.ctrl[kCtrlIter];
+    const unsigned char* prev = w.dirty[(it + 1) & 1];
+    unsigned char* cur = w.dirty[it & 1];
+    const bool force = w.ctrl[kCtrlForce] != 0;
+    const int nst = w.st_count[0];
+    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < g.n_outer; o += gridDim.x * blockDim.x) {
+        unsigned char nd = 1;
+        if (!force) {
+            nd = 0;
+            int co[32];
+            int rem = o;
+            for (int l = 0; l < g.od; l++) {
+                co[l] = rem % g.width;
+                rem /= g.width;
+            }
+            for (int s = 0; s < nst && !nd; s++) {
+                bool inb = true;
+                for (int l = 0; l < g.od; l++) {
+                    const int v = co[l] + __ldg(w.st_off + (size_t)s * g.od + l);
+                    inb = inb && (unsigned)v < (unsigned)g.width;
+                }
+                if (inb && prev[o + __ldg(w.st_delta + s)]) nd = 1;
+            }
+        }
+        w.need[o] = nd;
+        cur[o] = 0;
+    }
+}
+
+void launch_need(const Geom& g, const Work& w, cudaStream_t st) {
+    int blocks = (g.n_outer + 255) / 256;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    k_need<<<blocks, 256, 0, st>>>(g, w);
+}
 
 void launch_update(const Geom& g, const Work& w, int* counts, cudaStream_t st) {
     const int threads = 128;

@@ -28,7 +28,8 @@ EXPORTS = ("egg_opts_default", "egg_sync_run", "egg_sync_step", "egg_sync_grid",
 
 class EggOpts(C.Structure):
     _fields_ = [("max_iter", C.c_int32), ("loop", C.c_int32), ("stop_rule", C.c_int32),
-                ("order_param", C.c_int32), ("profile", C.c_int32), ("reserved", C.c_int32 * 11)]
+                ("order_param", C.c_int32), ("profile", C.c_int32), ("full_update", C.c_int32),
+                ("positions_out", C.c_void_p), ("reserved", C.c_int32 * 8)]
 
 
 class EggStats(C.Structure):

@@ -77,32 +77,44 @@ class _DeviceGuard:
             self.ctx.__exit__(*a)
 
 
+def _out_ptr(buf, n, dtype_np, what):
+    if isinstance(buf, np.ndarray):
+        if buf.dtype != dtype_np or buf.size != n or not buf.flags.c_contiguous:
+            raise ValueError("%s must be a contiguous %s array of %d entries" % (what, np.dtype(dtype_np), n))
+        return buf.ctypes.data
+    torch = _torch()
+    tdt = {np.int32: torch.int32, np.float32: torch.float32}[dtype_np]
+    if buf.dtype != tdt or buf.numel() != n or not buf.is_contiguous():
+        raise ValueError("%s must be a contiguous %s tensor of %d entries" % (what, tdt, n))
+    return buf.data_ptr()
+
+
 def egg_sync(D, eps: float, lam: float = DEFAULT_LAMBDA, max_iter: int = 0, loop: str = "graph",
-             labels_out=None, profile: bool = False) -> Tuple[object, dict]:
+             labels_out=None, profile: bool = False, full_update: bool = False,
+             positions_out=None) -> Tuple[object, dict]:
     """Run EGG-SynC; return (int32 labels, stats dict).
 
     ``labels_out`` may be a preallocated int32 numpy array or torch tensor
     (host or device) of n entries; by default a host numpy array is returned.
     ``loop`` is "graph" (device-resident loop) or "host".  ``profile`` times
-    every kernel group with CUDA events (host-driven loop)."""
+    every kernel group with CUDA events (host-driven loop).  ``full_update``
+    recomputes every point in every iteration (the default reuses results
+    whose inputs did not change; both give identical bits).
+    ``positions_out`` (optional n x d float32 buffer) receives the final
+    positions."""
     L = _lib.load()
     ptr, n, d, keep, dev, stream = _prepare(D)
     if labels_out is None:
         labels_out = np.empty(n, np.int32)
-    if isinstance(labels_out, np.ndarray):
-        if labels_out.dtype != np.int32 or labels_out.size != n or not labels_out.flags.c_contiguous:
-            raise ValueError("labels_out must be a contiguous int32 array of n entries")
-        lptr = labels_out.ctypes.data
-    else:
-        torch = _torch()
-        if labels_out.dtype != torch.int32 or labels_out.numel() != n or not labels_out.is_contiguous():
-            raise ValueError("labels_out must be a contiguous int32 tensor of n entries")
-        lptr = labels_out.data_ptr()
+    lptr = _out_ptr(labels_out, n, np.int32, "labels_out")
     opts = EggOpts()
     L.egg_opts_default(C.byref(opts))
     opts.max_iter = int(max_iter)
     opts.loop = {"graph": 0, "host": 1}[loop]
     opts.profile = 1 if profile else 0
+    opts.full_update = 1 if full_update else 0
+    if positions_out is not None:
+        opts.positions_out = _out_ptr(positions_out, n * d, np.float32, "positions_out")
     stats = EggStats()
     cap = opts.max_iter if opts.max_iter > 0 else 1000
     itr = (C.c_float * cap)()

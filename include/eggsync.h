@@ -40,7 +40,11 @@ typedef struct egg_opts {
                              1 = local order parameter >= lam (SynC.cpp:277-303 semantics) */
     int32_t order_param;  /* 0 = off, 1 = report the final FP64 order parameter */
     int32_t profile;      /* 1 = time every kernel group with CUDA events (host-driven loop) */
-    int32_t reserved[11];
+    int32_t full_update;  /* 1 = recompute every point in every iteration.  By default a point whose
+                             whole stencil region held no moved point since the last update keeps
+                             its previous result, which is bit-identical to recomputing it. */
+    float *positions_out; /* optional n x d buffer (host or device): final positions, input order */
+    int32_t reserved[8];
 } egg_opts;
 
 typedef struct egg_stats {

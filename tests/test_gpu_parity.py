@@ -100,6 +100,20 @@ def test_run_matches_reference_egg(name):
     assert info["iterations"] == int(G["iterations"][0])
 
 
+@pytest.mark.parametrize("name", ["c1_s0", "c3a_s0", "noise", "d5", "borders"])
+def test_incremental_equals_full_update(name):
+    """Reusing the results of points whose stencil region did not change is
+    bit-identical to recomputing every point in every iteration."""
+    X, eps = CASES[name]
+    pa = np.empty_like(X)
+    pb = np.empty_like(X)
+    la, ia = egg_sync(X, eps, positions_out=pa)
+    lb, ib = egg_sync(X, eps, full_update=True, positions_out=pb)
+    assert ia["iterations"] == ib["iterations"]
+    assert np.array_equal(la, lb)
+    assert np.array_equal(pa.view(np.uint32), pb.view(np.uint32))
+
+
 def test_deterministic_and_loop_modes():
     X, eps = CASES["c1_s0"]
     a, ia = egg_sync(X, eps)
@@ -175,8 +189,18 @@ def test_large_run_properties():
     one final cell; a second run is identical."""
     c = data.c5(0)
     X, eps = c["X"], c["eps"]
-    lab, info = egg_sync(X, eps)
+    pa = np.empty_like(X)
+    lab, info = egg_sync(X, eps, positions_out=pa)
     assert info["converged"] and info["iterations"] > 1
     assert info["n_clusters"] == len(np.unique(lab[lab >= 0]))
-    lab2, info2 = egg_sync(X, eps)
+    # the labels are exactly the final grid's cells holding > 1 point
+    order, cell_of, start = egg_grid(pa, eps)
+    size = np.diff(start)[cell_of]
+    lab_sorted = np.where(size > 1, cell_of, -1)
+    assert np.array_equal(lab[order], lab_sorted)
+    # a second run, and a run that recomputes every point every iteration,
+    # give the same bits
+    pb = np.empty_like(X)
+    lab2, info2 = egg_sync(X, eps, full_update=True, positions_out=pb)
     assert np.array_equal(lab, lab2) and info2["iterations"] == info["iterations"]
+    assert np.array_equal(pa.view(np.uint32), pb.view(np.uint32))
