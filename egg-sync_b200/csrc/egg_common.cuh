@@ -96,6 +96,7 @@ struct Work {
     unsigned char* dirty[2];   // [n_outer]
     unsigned char* need;       // [n_outer]
     unsigned char* viol_orig;  // [ns] by original index
+    int* span_list;            // [ns/32 + 1] cells whose points span several warps
 };
 
 enum : int {
@@ -114,6 +115,7 @@ enum : int {
     kCtrlForce = 12,      // recompute every point (first iteration of a run)
     kCtrlComputed = 13,   // points recomputed by the update (statistics)
     kCtrlFullUpdate = 14, // recompute every point in every iteration
+    kCtrlSpanCount = 15,  // cells listed in span_list by the cell-sums kernel
 };
 
 // ------------------------------------------------------------------------

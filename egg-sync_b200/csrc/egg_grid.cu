@@ -90,7 +90,10 @@ __global__ void __launch_bounds__(256) k_check_cells(Geom g, Work w) {
     if (__syncthreads_or(changed) && threadIdx.x == 0) w.ctrl[kCtrlChanged] = 1;
 }
 
-__global__ void k_build_begin(int* ctrl) { ctrl[kCtrlChanged] = 0; }
+__global__ void k_build_begin(int* ctrl) {
+    ctrl[kCtrlChanged] = 0;
+    ctrl[kCtrlSpanCount] = 0;
+}
 
 #define EGG_SKIP_IF_UNCHANGED(ctrl) \
     if ((ctrl)[kCtrlChanged] == 0) return;
@@ -330,7 +333,9 @@ __global__ void __launch_bounds__(256) k_cell_sums(Geom g, Work w) {
         ce = w.cell_start[c + 1];
     }
     const bool complete = seg_end && cs >= wb && ce <= wb + 32;
-    // segment start lane: for the record of the first segment
+    // a cell that starts in this warp and continues past it: list it once
+    // for the FP64 combination of its warp partials
+    if (seg_end && cs >= wb && ce > wb + 32) w.span_list[atomicAdd(w.ctrl + kCtrlSpanCount, 1)] = c;
     for (int l = 0; l < d; l++) {
         float s = 0.f, m = 0.f, x = 0.f;
         if (valid) {
@@ -391,51 +396,74 @@ __global__ void __launch_bounds__(256) k_cell_sums(Geom g, Work w) {
 }
 
 // Cells spanning more than one warp (the heavily populated ones): combine the
-// warp partials in FP64 in a fixed order.  One warp per 32 cells.
+// warp partials in FP64 in a fixed order, one warp per listed cell.  The list
+// order depends on scheduling, the result of every cell does not.
+template <int D>
 __global__ void __launch_bounds__(256) k_cell_sums_fix(Geom g, Work w) {
-    const int M = w.ctrl[kCtrlM];
+    constexpr int DM = D > 0 ? D : 1;
+    const int d = D > 0 ? D : g.d;
     const int lane = threadIdx.x & 31;
-    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int c0 = gw * 32;
-    if (c0 >= M) return;
+    const int count = w.ctrl[kCtrlSpanCount];
     const int nw = (g.n + 31) >> 5;
-    const int c = c0 + lane;
-    int cs = 0, ce = 0;
-    bool span = false;
-    if (c < M) {
-        cs = w.cell_start[c];
-        ce = w.cell_start[c + 1];
-        span = (cs >> 5) != ((ce - 1) >> 5);
-    }
-    unsigned todo = __ballot_sync(0xffffffffu, span);
-    while (todo) {
-        const int src = __ffs(todo) - 1;
-        todo &= todo - 1;
-        const int cc = c0 + src;
-        const int scs = __shfl_sync(0xffffffffu, cs, src);
-        const int sce = __shfl_sync(0xffffffffu, ce, src);
-        const int wh = scs >> 5, wt = (sce - 1) >> 5;
-        for (int l = 0; l < g.d; l++) {
-            double S = 0.0, Mm = 0.0, mn = 1e300, mx = -1e300;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < count; e += warps) {
+        const int c = w.span_list[e];
+        const int cs = w.cell_start[c], ce = w.cell_start[c + 1];
+        const int wh = cs >> 5, wt = (ce - 1) >> 5;
+        if (D > 0) {
+            // every dimension in one pass: 4*D independent loads per partial
+            double S[DM], Mm[DM], mn[DM], mx[DM];
+#pragma unroll
+            for (int l = 0; l < DM; l++) { S[l] = 0.0; Mm[l] = 0.0; mn[l] = 1e300; mx[l] = -1e300; }
             for (int k = wh + lane; k <= wt; k += 32) {
                 const int rec = (k == wh) ? 1 : 0;
-                S += w.wpart[wp_idx(0, l, g.d, rec, nw, k)];
-                Mm += w.wpart[wp_idx(1, l, g.d, rec, nw, k)];
-                mn = fmin(mn, w.wpart[wp_idx(2, l, g.d, rec, nw, k)]);
-                mx = fmax(mx, w.wpart[wp_idx(3, l, g.d, rec, nw, k)]);
+#pragma unroll
+                for (int l = 0; l < DM; l++) {
+                    S[l] += w.wpart[wp_idx(0, l, d, rec, nw, k)];
+                    Mm[l] += w.wpart[wp_idx(1, l, d, rec, nw, k)];
+                    mn[l] = fmin(mn[l], w.wpart[wp_idx(2, l, d, rec, nw, k)]);
+                    mx[l] = fmax(mx[l], w.wpart[wp_idx(3, l, d, rec, nw, k)]);
+                }
             }
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                S += __shfl_xor_sync(0xffffffffu, S, o);
-                Mm += __shfl_xor_sync(0xffffffffu, Mm, o);
-                mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-                mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            for (int l = 0; l < DM; l++) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    S[l] += __shfl_xor_sync(0xffffffffu, S[l], o);
+                    Mm[l] += __shfl_xor_sync(0xffffffffu, Mm[l], o);
+                    mn[l] = fmin(mn[l], __shfl_xor_sync(0xffffffffu, mn[l], o));
+                    mx[l] = fmax(mx[l], __shfl_xor_sync(0xffffffffu, mx[l], o));
+                }
+                if (lane == 0) {
+                    w.css[(size_t)l * g.ns + c] = (float)S[l];
+                    w.csm[(size_t)l * g.ns + c] = (float)Mm[l];
+                    w.cbmin[(size_t)l * g.ns + c] = (float)mn[l];
+                    w.cbmax[(size_t)l * g.ns + c] = (float)mx[l];
+                }
             }
-            if (lane == 0) {
-                w.css[(size_t)l * g.ns + cc] = (float)S;
-                w.csm[(size_t)l * g.ns + cc] = (float)Mm;
-                w.cbmin[(size_t)l * g.ns + cc] = (float)mn;
-                w.cbmax[(size_t)l * g.ns + cc] = (float)mx;
+        } else {
+            for (int l = 0; l < d; l++) {
+                double S = 0.0, Mm = 0.0, mn = 1e300, mx = -1e300;
+                for (int k = wh + lane; k <= wt; k += 32) {
+                    const int rec = (k == wh) ? 1 : 0;
+                    S += w.wpart[wp_idx(0, l, d, rec, nw, k)];
+                    Mm += w.wpart[wp_idx(1, l, d, rec, nw, k)];
+                    mn = fmin(mn, w.wpart[wp_idx(2, l, d, rec, nw, k)]);
+                    mx = fmax(mx, w.wpart[wp_idx(3, l, d, rec, nw, k)]);
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    S += __shfl_xor_sync(0xffffffffu, S, o);
+                    Mm += __shfl_xor_sync(0xffffffffu, Mm, o);
+                    mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+                    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+                }
+                if (lane == 0) {
+                    w.css[(size_t)l * g.ns + c] = (float)S;
+                    w.csm[(size_t)l * g.ns + c] = (float)Mm;
+                    w.cbmin[(size_t)l * g.ns + c] = (float)mn;
+                    w.cbmax[(size_t)l * g.ns + c] = (float)mx;
+                }
             }
         }
     }
@@ -535,8 +563,9 @@ void launch_build(const Geom& g, const Work& w, const SortPlan& plan, cudaStream
 void launch_cell_sums(const Geom& g, const Work& w, cudaStream_t st) {
     const int blocks = (g.n + 255) / 256;
     EGG_DISPATCH_D(g.d, k_cell_sums, <<<blocks, 256, 0, st>>>(g, w));
-    const int fix_warps = (g.n + 31) / 32;
-    k_cell_sums_fix<<<(fix_warps * 32 + 255) / 256, 256, 0, st>>>(g, w);
+    int fix_blocks = ((g.n + 31) / 32 + 7) / 8;  // one warp per possible spanning cell
+    if (fix_blocks > 148 * 8) fix_blocks = 148 * 8;
+    EGG_DISPATCH_D(g.d, k_cell_sums_fix, <<<fix_blocks, 256, 0, st>>>(g, w));
 }
 
 void launch_transpose_in(const Geom& g, const Work& w, const float* x, cudaStream_t st) {

@@ -263,6 +263,7 @@ void prepare(Instance& I, const Geom& g, int max_iter) {
     add((void**)&w.dirty[1], (size_t)g.n_outer + 1);
     add((void**)&w.need, (size_t)g.n_outer + 1);
     add((void**)&w.viol_orig, ns);
+    add((void**)&w.span_list, 4 * ((size_t)nw + 1));
     for (auto& p : plan) off += align_up(p.second);
     if (off > I.cap) {
         destroy_graph(I);
