@@ -46,6 +46,8 @@ struct Geom {
     float t_eps;       // largest v with sqrtf(v) <= eps
     float t_half;      // ... <= eps/2
     float t_extra;     // ... <= eps_extra
+    int sub_dims;      // dimensions in the within-cell (sub-cell) sort key
+    int sub_bits;      // bits per dimension of the sub-cell key (sub_dims*sub_bits <= 8)
     int wpow[32];      // width^l for l < od
 };
 
@@ -78,6 +80,7 @@ struct Work {
     int* digit_total;  // [256]
     int* block_sums;   // [blocks]
     double* wpart;     // [(2d values + 2d bbox) * 2 * warps] warp partials for spanning cells
+    float* gpart;      // the same records in FP32: the 32-point groups of spanning cells
     // stencils (host-built tables)
     int* st_delta;     // [3][st_cap] linear outer-id offset
     signed char* st_off;  // [3][st_cap * od] per-dimension offsets
@@ -193,6 +196,13 @@ __device__ __forceinline__ void tight_box_dist2(const float* x, const float* __r
     }
     near2 = a2;
     far2 = b2;
+}
+
+// index of a warp-partial record: ((field * d + l) * 2 + rec) * warps + warp,
+// field in {sum sin, sum 1-cos, min, max}; rec 0 = the segment holding the
+// warp's lane 0, rec 1 = the segment holding lane 31
+__device__ __forceinline__ size_t wp_idx_f(int field, int l, int d, int rec, int nw, int warp) {
+    return ((size_t)(field * d + l) * 2 + rec) * nw + warp;
 }
 
 __device__ __forceinline__ unsigned long long globaltimer() {

@@ -60,9 +60,30 @@ __device__ int block_exclusive_scan(int v, int* total) {
     return excl;
 }
 
+// Sort digit of point j.  dim >= 0: bits [shift, shift+8) of the point's cell
+// index in that dimension.  dim < 0: the sub-cell key, a Morton interleave of
+// the top sub_bits bits of the point's offset inside its cell in the first
+// sub_dims dimensions; sorted first (least significant), it orders the points
+// of every cell along a space-filling curve, so consecutive runs of a cell's
+// points (its 32-point groups) are spatially compact.
 __device__ __forceinline__ int digit_of(const Geom& g, const float* __restrict__ Xs, int j, int dim, int shift) {
-    float x = __ldg(Xs + (size_t)dim * g.ns + j);
-    return (cell_dim(x, g) >> shift) & 255;
+    if (dim >= 0) {
+        float x = __ldg(Xs + (size_t)dim * g.ns + j);
+        return (cell_dim(x, g) >> shift) & 255;
+    }
+    const int b = g.sub_bits;
+    const float scale = (float)(1 << b) / g.side;
+    int t[8];
+    for (int l = 0; l < g.sub_dims; l++) {
+        const float x = __ldg(Xs + (size_t)l * g.ns + j);
+        const float off = x - __fmul_rn((float)cell_dim(x, g), g.side);
+        int v = (int)(off * scale);
+        t[l] = v < 0 ? 0 : (v > (1 << b) - 1 ? (1 << b) - 1 : v);
+    }
+    int dig = 0;
+    for (int k = b - 1; k >= 0; k--)
+        for (int l = 0; l < g.sub_dims; l++) dig = (dig << 1) | ((t[l] >> k) & 1);
+    return dig;
 }
 
 }  // namespace
@@ -87,6 +108,8 @@ __global__ void __launch_bounds__(256) k_check_cells(Geom g, Work w) {
         }
     }
     if (!valid) changed = true;
+    // the incremental update's need marks are rebuilt after every grid check
+    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < g.n_outer; o += gridDim.x * blockDim.x) w.need[o] = 0;
     if (__syncthreads_or(changed) && threadIdx.x == 0) w.ctrl[kCtrlChanged] = 1;
 }
 
@@ -376,19 +399,21 @@ __global__ void __launch_bounds__(256) k_cell_sums(Geom g, Work w) {
             // lane 0 (continues from the previous warp), rec 1 = segment holding
             // lane 31 (continues into the next warp); a warp inside one cell
             // writes both.
+            // The FP32 copy (gpart) is the record of this 32-point group of
+            // the cell, used by the update to decide groups wholesale.
             const double S = (double)vs.hi + (double)vs.lo;
             const double Mm = (double)vm.hi + (double)vm.lo;
-            if (cs < wb) {
-                w.wpart[wp_idx(0, l, d, 0, nw, warp)] = S;
-                w.wpart[wp_idx(1, l, d, 0, nw, warp)] = Mm;
-                w.wpart[wp_idx(2, l, d, 0, nw, warp)] = mn;
-                w.wpart[wp_idx(3, l, d, 0, nw, warp)] = mx;
-            }
-            if (ce > wb + 32) {
-                w.wpart[wp_idx(0, l, d, 1, nw, warp)] = S;
-                w.wpart[wp_idx(1, l, d, 1, nw, warp)] = Mm;
-                w.wpart[wp_idx(2, l, d, 1, nw, warp)] = mn;
-                w.wpart[wp_idx(3, l, d, 1, nw, warp)] = mx;
+            const float Sf = __fadd_rn(vs.hi, vs.lo), Mf = __fadd_rn(vm.hi, vm.lo);
+            for (int rec = 0; rec < 2; rec++) {
+                if (rec == 0 ? !(cs < wb) : !(ce > wb + 32)) continue;
+                w.wpart[wp_idx(0, l, d, rec, nw, warp)] = S;
+                w.wpart[wp_idx(1, l, d, rec, nw, warp)] = Mm;
+                w.wpart[wp_idx(2, l, d, rec, nw, warp)] = mn;
+                w.wpart[wp_idx(3, l, d, rec, nw, warp)] = mx;
+                w.gpart[wp_idx(0, l, d, rec, nw, warp)] = Sf;
+                w.gpart[wp_idx(1, l, d, rec, nw, warp)] = Mf;
+                w.gpart[wp_idx(2, l, d, rec, nw, warp)] = mn;
+                w.gpart[wp_idx(3, l, d, rec, nw, warp)] = mx;
             }
         }
     }

@@ -102,6 +102,8 @@ Geom make_geom(int64_t n64, int d, float eps) {
     g.t_extra = sq_threshold(g.eps_extra);
     g.table_k = std::max(g.r, std::max(g.r_extra, g.r_half)) + 2;
     if (g.table_k > kMaxTable) throw ArgError{EGG_ERR_GEOMETRY, "stencil radius too large"};
+    g.sub_dims = std::min(d, 8);
+    g.sub_bits = std::max(1, 8 / g.sub_dims);
     return g;
 }
 
@@ -117,7 +119,11 @@ SortPlan make_plan(const Geom& g) {
             P.count++;
         }
     };
-    // least significant first: g_{d-1}, ..., g_od, then g_0, ..., g_{od-1}
+    // least significant first: the sub-cell key (order inside a cell), then
+    // g_{d-1}, ..., g_od, then g_0, ..., g_{od-1}
+    P.dim[P.count] = -1;
+    P.shift[P.count] = 0;
+    P.count++;
     for (int l = g.d - 1; l >= g.od; l--) add_dim(l);
     for (int l = 0; l < g.od; l++) add_dim(l);
     return P;
@@ -251,6 +257,7 @@ void prepare(Instance& I, const Geom& g, int max_iter) {
     add((void**)&w.digit_total, 4 * 256);
     add((void**)&w.block_sums, 4 * (size_t)nb);
     add((void**)&w.wpart, 8 * 4 * (size_t)d * 2 * nw);
+    add((void**)&w.gpart, 4 * 4 * (size_t)d * 2 * nw);
     add((void**)&w.st_delta, 4 * 3 * (size_t)st_cap);
     add((void**)&w.st_off, 3 * (size_t)st_cap * odp);
     add((void**)&w.table, 4 * 3 * (size_t)TW);
@@ -441,6 +448,8 @@ void load_input(Instance& I, const float* x, int full_update = 0) {
         src = I.xin;
     }
     k_ctrl_reset<<<1, 32, 0, I.st>>>(I.w, I.max_iter, full_update);
+    EGG_CHECK(cudaMemsetAsync(I.w.dirty[0], 0, (size_t)g.n_outer + 1, I.st));
+    EGG_CHECK(cudaMemsetAsync(I.w.dirty[1], 0, (size_t)g.n_outer + 1, I.st));
     launch_transpose_in(g, I.w, src, I.st);
 }
 

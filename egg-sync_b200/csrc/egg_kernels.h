@@ -8,11 +8,12 @@
 namespace egg {
 
 // LSD radix passes over the cell digits: pass p sorts on
-// (cell_dim(x[dim[p]]) >> shift[p]) & 255, least significant pass first.
+// (cell_dim(x[dim[p]]) >> shift[p]) & 255, least significant pass first;
+// dim[p] < 0 is the within-cell sub-cell key.
 struct SortPlan {
     int count = 0;
-    int dim[2 * kMaxDims];
-    int shift[2 * kMaxDims];
+    int dim[2 * kMaxDims + 1];
+    int shift[2 * kMaxDims + 1];
 };
 
 // grid (egg_grid.cu)

@@ -140,15 +140,43 @@ __device__ __forceinline__ void visit_cell(const Geom& g, const Work& w, int c, 
     float as[DM], am[DM];
     for (int l = 0; l < d; l++) { as[l] = 0.f; am[l] = 0.f; }
     int cnt = 0;
-    for (int q = qb; q < qe; q++) {
-        float d2 = 0.f;
-        for (int l = 0; l < d; l++) d2 = dist_step(__ldg(w.X + (size_t)l * g.ns + q), x[l], d2);
-        if (d2 <= g.t_eps) {
+    const int kh = qb >> 5, kt = (qe - 1) >> 5;
+    for (int k = kh; k <= kt; k++) {
+        // the cell's points in warp k: one 32-point group of a cell ordered
+        // along the sub-cell curve; its tight box decides it wholesale when
+        // all or none of its points are within eps
+        const int sb = max(qb, k << 5), se = min(qe, (k << 5) + 32);
+        if (kh != kt) {
+            const int nw = (g.n + 31) >> 5;
+            const int rec = (k == kh) ? 1 : 0;
+            float n2 = 0.f, f2 = 0.f;
             for (int l = 0; l < d; l++) {
-                as[l] += __ldg(w.sd + (size_t)l * g.ns + q);
-                am[l] += __ldg(w.md + (size_t)l * g.ns + q);
+                const float L = __ldg(w.gpart + wp_idx_f(2, l, d, rec, nw, k));
+                const float H = __ldg(w.gpart + wp_idx_f(3, l, d, rec, nw, k));
+                const float a0 = near_gap(x[l], L, H), b0 = far_gap(x[l], L, H);
+                n2 = __fmaf_rn(a0, a0, n2);
+                f2 = __fmaf_rn(b0, b0, f2);
             }
-            cnt++;
+            if (n2 > g.t_eps) continue;
+            if (f2 <= g.t_eps) {
+                for (int l = 0; l < d; l++) {
+                    as[l] += __ldg(w.gpart + wp_idx_f(0, l, d, rec, nw, k));
+                    am[l] += __ldg(w.gpart + wp_idx_f(1, l, d, rec, nw, k));
+                }
+                cnt += se - sb;
+                continue;
+            }
+        }
+        for (int q = sb; q < se; q++) {
+            float d2 = 0.f;
+            for (int l = 0; l < d; l++) d2 = dist_step(__ldg(w.X + (size_t)l * g.ns + q), x[l], d2);
+            if (d2 <= g.t_eps) {
+                for (int l = 0; l < d; l++) {
+                    as[l] += __ldg(w.sd + (size_t)l * g.ns + q);
+                    am[l] += __ldg(w.md + (size_t)l * g.ns + q);
+                }
+                cnt++;
+            }
         }
     }
     if (cnt) {
@@ -351,36 +379,31 @@ __global__ void __launch_bounds__(128) k_update(Geom g, Work w, int* __restrict_
         default: KERNEL<0> __VA_ARGS__; break;        \
     }
 
-// need[o] = some outer cell of o's stencil holds a point that moved in the
-// last update (dirty of the previous iteration); also clears the dirty marks
-// the coming update will write.
+// need[] (zeroed by the grid-build check of this iteration) is set over the
+// stencil of every outer cell that the previous update marked dirty (a moved
+// point's old or new position); the marks are cleared as they are consumed,
+// so the array is clean again when the update after next writes it.
 __global__ void k_need(Geom g, Work w) {
     const int it = w.ctrl[kCtrlIter];
-    const unsigned char* prev = w.dirty[(it + 1) & 1];
-    unsigned char* cur = w.dirty[it & 1];
-    const bool force = w.ctrl[kCtrlForce] != 0;
+    unsigned char* prev = w.dirty[(it + 1) & 1];
     const int nst = w.st_count[0];
     for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < g.n_outer; o += gridDim.x * blockDim.x) {
-        unsigned char nd = 1;
-        if (!force) {
-            nd = 0;
-            int co[32];
-            int rem = o;
-            for (int l = 0; l < g.od; l++) {
-                co[l] = rem % g.width;
-                rem /= g.width;
-            }
-            for (int s = 0; s < nst && !nd; s++) {
-                bool inb = true;
-                for (int l = 0; l < g.od; l++) {
-                    const int v = co[l] + __ldg(w.st_off + (size_t)s * g.od + l);
-                    inb = inb && (unsigned)v < (unsigned)g.width;
-                }
-                if (inb && prev[o + __ldg(w.st_delta + s)]) nd = 1;
-            }
+        if (!prev[o]) continue;
+        prev[o] = 0;
+        int co[32];
+        int rem = o;
+        for (int l = 0; l < g.od; l++) {
+            co[l] = rem % g.width;
+            rem /= g.width;
         }
-        w.need[o] = nd;
-        cur[o] = 0;
+        for (int s = 0; s < nst; s++) {
+            bool inb = true;
+            for (int l = 0; l < g.od; l++) {
+                const int v = co[l] + __ldg(w.st_off + (size_t)s * g.od + l);
+                inb = inb && (unsigned)v < (unsigned)g.width;
+            }
+            if (inb) w.need[o + __ldg(w.st_delta + s)] = 1;
+        }
     }
 }
 

@@ -196,6 +196,7 @@ typedef struct {
     const float *X;      /* n*d row-major */
     int *gid;            /* n*d dim ids per point */
     int64_t *outer;      /* per point outer id */
+    int *sub;            /* per point sub-cell key (order inside a cell) */
     int *order;          /* sorted position -> point */
     int *cell_of_pt;     /* point -> cell */
     int M;               /* number of non-empty cells */
@@ -214,7 +215,28 @@ static int cmp_points(const void *pa, const void *pb) {
         int ga = G->gid[(size_t)a * G->d + l], gb = G->gid[(size_t)b * G->d + l];
         if (ga != gb) return ga < gb ? -1 : 1;
     }
+    if (G->sub[a] != G->sub[b]) return G->sub[a] < G->sub[b] ? -1 : 1;
     return a < b ? -1 : (a > b);
+}
+
+/* Order of the points inside a cell (the GPU path's choice, not the
+ * reference's; it only changes summation order): a Morton interleave of the
+ * top `bits` bits of the point's offset inside its cell in the first
+ * min(d, 8) dimensions, bits = max(1, 8 / min(d, 8)). */
+static int sub_key(const float *x, const int *gid, const egg_geom *g) {
+    const int nd = g->d < 8 ? g->d : 8;
+    const int b = 8 / nd > 1 ? 8 / nd : 1;
+    const float scale = (float)(1 << b) / g->side;
+    int t[8];
+    for (int l = 0; l < nd; l++) {
+        const float off = x[l] - (float)gid[l] * g->side;
+        int v = (int)(off * scale);
+        t[l] = v < 0 ? 0 : (v > (1 << b) - 1 ? (1 << b) - 1 : v);
+    }
+    int dig = 0;
+    for (int k = b - 1; k >= 0; k--)
+        for (int l = 0; l < nd; l++) dig = (dig << 1) | ((t[l] >> k) & 1);
+    return dig;
 }
 
 static int grid_build(grid_t *G, const float *X, int n, int d, float eps) {
@@ -223,6 +245,7 @@ static int grid_build(grid_t *G, const float *X, int n, int d, float eps) {
     G->n = n; G->d = d; G->X = X;
     G->gid = (int *)malloc(sizeof(int) * (size_t)n * d);
     G->outer = (int64_t *)malloc(sizeof(int64_t) * (size_t)n);
+    G->sub = (int *)malloc(sizeof(int) * (size_t)n);
     G->order = (int *)malloc(sizeof(int) * (size_t)n);
     G->cell_of_pt = (int *)malloc(sizeof(int) * (size_t)n);
     G->cell_start = (int *)malloc(sizeof(int) * ((size_t)n + 1));
@@ -237,6 +260,7 @@ static int grid_build(grid_t *G, const float *X, int n, int d, float eps) {
             if (l < G->g.od) { o += (int64_t)t * mul; mul *= G->g.width; }
         }
         G->outer[p] = o;
+        G->sub[p] = sub_key(&X[(size_t)p * d], &G->gid[(size_t)p * d], &G->g);
         G->order[p] = p;
     }
     g_sort_ctx = G;
@@ -270,7 +294,7 @@ static int grid_build(grid_t *G, const float *X, int n, int d, float eps) {
 }
 
 static void grid_free(grid_t *G) {
-    free(G->gid); free(G->outer); free(G->order); free(G->cell_of_pt);
+    free(G->gid); free(G->outer); free(G->sub); free(G->order); free(G->cell_of_pt);
     free(G->cell_start); free(G->cell_dims); free(G->cell_outer); free(G->outer_begin);
 }
 

@@ -96,9 +96,17 @@ def test_grid_structure(oracle):
     eps = 0.05
     order, cell_of, start = oracle.grid(X, eps)
     g = oracle.geometry(len(X), 3, eps)
-    ids = np.minimum((X / np.float32(g.side)).astype(np.int64), g.width - 1)
+    side = np.float32(g.side)
+    ids = np.minimum((X / side).astype(np.int64), g.width - 1)
     outer = sum(ids[:, l] * g.width ** l for l in range(g.od))
-    key = [outer] + [ids[:, l] for l in range(g.od, 3)]
+    # within-cell order: Morton key of the top 2 bits of the in-cell offsets (d = 3)
+    scale = np.float32(4) / side
+    t = np.clip(((X - ids.astype(np.float32) * side) * scale).astype(np.int64), 0, 3)
+    sub = np.zeros(len(X), np.int64)
+    for k in (1, 0):
+        for l in range(3):
+            sub = (sub << 1) | ((t[:, l] >> k) & 1)
+    key = [outer] + [ids[:, l] for l in range(g.od, 3)] + [sub]
     ref = np.lexsort(tuple([np.arange(len(X))] + key[::-1]))
     assert np.array_equal(order, ref)
     # every cell is a run of identical tuples, runs are maximal
