@@ -61,6 +61,8 @@ struct Work {
     float* md;         // [d][ns] 1 - cos(delta) (= 2 sin^2(delta/2))
     float* qlo;        // [d][ns] eps/2-ball extremes (extra check)
     float* qhi;        // [d][ns]
+    float* ulo;        // [d][ns] per cell: union of its points' eps/2-ball extremes
+    float* uhi;        // [d][ns]
     int* orig;         // [ns]   original index of sorted point i
     int* orig_tmp;     // [ns]
     int* perm;         // [ns]   radix sort output: new position -> previous position
@@ -132,10 +134,17 @@ __device__ __forceinline__ int cell_dim(float x, const Geom& g) {
     return t;
 }
 
-// reference border rule, EGG_SynC.cu:590-596 (the +-1e-5 probes are double)
+// reference border rule, EGG_SynC.cu:590-596 (the +-1e-5 probes are double).
+// A point whose cell coordinate x/side is farther than 1e-5/side from every
+// integer, with margins for the float rounding of x/side, gives
+// idm == id == idp; only points near a face take the exact double path.
 __device__ __forceinline__ bool on_border_dim(float x, float side) {
+    const float q = __fdiv_rn(x, side);
+    const int id = (int)q;
+    const float f = q - floorf(q);
+    const float a = 1.001e-5f / side + 2.5e-7f * fabsf(q) + 1e-6f;
+    if (q >= 0.0f && f > a && f < 1.0f - a) return false;
     int idm = (int)__ddiv_rn((double)x - 0.00001, (double)side);
-    int id = (int)__fdiv_rn(x, side);
     int idp = (int)__ddiv_rn((double)x + 0.00001, (double)side);
     return (id != idm) || (id != idp);
 }

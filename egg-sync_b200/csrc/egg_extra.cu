@@ -105,48 +105,69 @@ __global__ void __launch_bounds__(128) k_ball_bbox(Geom g, Work w) {
         w.stamps[4 * it + 2] = globaltimer();
     }
     if (w.ctrl[kCtrlFlag] == 0) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.n) return;
-    float xq[DM], lo[DM], hi[DM];
-    int gq[DM];
-    int obase = 0;
-    for (int l = 0; l < d; l++) {
-        xq[l] = w.X[(size_t)l * g.ns + i];
-        lo[l] = hi[l] = xq[l];
-        gq[l] = cell_dim(xq[l], g);
-        if (l < g.od) obase += gq[l] * g.wpow[l];
-    }
-    for_stencil_cells(g, w, 2, g.r_half, gq, obase, d, [&](int c) {
-        float sm2 = 0.f, lg2 = 0.f;
-        for (int l = 0; l < d; l++) box_terms(xq[l], __ldg(w.cell_dims + (size_t)l * g.ns + c), g.side, sm2, lg2);
-        if (!(sm2 <= g.t_half)) return true;
-        // none / all of the cell's points inside the eps/2 ball?
-        float near2, far2;
-        tight_box_dist2(xq, w.cbmin + c, w.cbmax + c, g.ns, d, near2, far2);
-        if (near2 > g.t_half) return true;
-        if (far2 <= g.t_half) {
-            for (int l = 0; l < d; l++) {
-                lo[l] = fminf(lo[l], __ldg(w.cbmin + (size_t)l * g.ns + c));
-                hi[l] = fmaxf(hi[l], __ldg(w.cbmax + (size_t)l * g.ns + c));
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+        float xq[DM], lo[DM], hi[DM];
+        int gq[DM];
+        int obase = 0;
+        for (int l = 0; l < d; l++) {
+            xq[l] = w.X[(size_t)l * g.ns + i];
+            lo[l] = hi[l] = xq[l];
+            gq[l] = cell_dim(xq[l], g);
+            if (l < g.od) obase += gq[l] * g.wpow[l];
+        }
+        for_stencil_cells(g, w, 2, g.r_half, gq, obase, d, [&](int c) {
+            float sm2 = 0.f, lg2 = 0.f;
+            for (int l = 0; l < d; l++)
+                box_terms(xq[l], __ldg(w.cell_dims + (size_t)l * g.ns + c), g.side, sm2, lg2);
+            if (!(sm2 <= g.t_half)) return true;
+            // none / all of the cell's points inside the eps/2 ball?
+            float near2, far2;
+            tight_box_dist2(xq, w.cbmin + c, w.cbmax + c, g.ns, d, near2, far2);
+            if (near2 > g.t_half) return true;
+            if (far2 <= g.t_half) {
+                for (int l = 0; l < d; l++) {
+                    lo[l] = fminf(lo[l], __ldg(w.cbmin + (size_t)l * g.ns + c));
+                    hi[l] = fmaxf(hi[l], __ldg(w.cbmax + (size_t)l * g.ns + c));
+                }
+                return true;
+            }
+            const int qb = __ldg(w.cell_start + c), qe = __ldg(w.cell_start + c + 1);
+            for (int r = qb; r < qe; r++) {
+                float d2 = 0.f;
+                for (int l = 0; l < d; l++) d2 = dist_step(xq[l], __ldg(w.X + (size_t)l * g.ns + r), d2);
+                if (d2 <= g.t_half)
+                    for (int l = 0; l < d; l++) {
+                        const float v = __ldg(w.X + (size_t)l * g.ns + r);
+                        lo[l] = fminf(lo[l], v);
+                        hi[l] = fmaxf(hi[l], v);
+                    }
             }
             return true;
+        });
+        for (int l = 0; l < d; l++) {
+            w.qlo[(size_t)l * g.ns + i] = lo[l];
+            w.qhi[(size_t)l * g.ns + i] = hi[l];
         }
-        const int qb = __ldg(w.cell_start + c), qe = __ldg(w.cell_start + c + 1);
-        for (int r = qb; r < qe; r++) {
-            float d2 = 0.f;
-            for (int l = 0; l < d; l++) d2 = dist_step(xq[l], __ldg(w.X + (size_t)l * g.ns + r), d2);
-            if (d2 <= g.t_half)
-                for (int l = 0; l < d; l++) {
-                    const float v = __ldg(w.X + (size_t)l * g.ns + r);
-                    lo[l] = fminf(lo[l], v);
-                    hi[l] = fmaxf(hi[l], v);
-                }
+    }
+}
+
+// Union over a cell's points of their eps/2-group extremes.  The MBR of any
+// pair (p, q) with q in the cell lies inside it, so its distance to p is a
+// lower bound for every pair of the cell.
+__global__ void __launch_bounds__(256) k_cell_ballbox(Geom g, Work w) {
+    if (w.ctrl[kCtrlFlag] == 0) return;
+    const int M = w.ctrl[kCtrlM];
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < M; c += gridDim.x * blockDim.x) {
+        const int qb = w.cell_start[c], qe = w.cell_start[c + 1];
+        for (int l = 0; l < g.d; l++) {
+            float lo = 3.0e38f, hi = -3.0e38f;
+            for (int q = qb; q < qe; q++) {
+                lo = fminf(lo, w.qlo[(size_t)l * g.ns + q]);
+                hi = fmaxf(hi, w.qhi[(size_t)l * g.ns + q]);
+            }
+            w.ulo[(size_t)l * g.ns + c] = lo;
+            w.uhi[(size_t)l * g.ns + c] = hi;
         }
-        return true;
-    });
-    for (int l = 0; l < d; l++) {
-        w.qlo[(size_t)l * g.ns + i] = lo[l];
-        w.qhi[(size_t)l * g.ns + i] = hi[l];
     }
 }
 
@@ -156,55 +177,59 @@ __global__ void __launch_bounds__(128) k_annulus(Geom g, Work w) {
     const int d = D > 0 ? D : g.d;
     volatile int* flag = w.ctrl + kCtrlFlag;
     if (*flag == 0) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.n) return;
-    float xp[DM];
-    int gp[DM];
-    int obase = 0;
-    for (int l = 0; l < d; l++) {
-        xp[l] = w.X[(size_t)l * g.ns + i];
-        gp[l] = cell_dim(xp[l], g);
-        if (l < g.od) obase += gp[l] * g.wpow[l];
-    }
     int pairs = 0;
-    bool violated = false;
-    for_stencil_cells(g, w, 1, g.r_extra, gp, obase, d, [&](int c) {
-        if (*flag == 0) return false;
-        float sm2 = 0.f, lg2 = 0.f;
-        for (int l = 0; l < d; l++) box_terms(xp[l], __ldg(w.cell_dims + (size_t)l * g.ns + c), g.side, sm2, lg2);
-        const bool included = sm2 <= g.t_extra;
-        const bool fully = lg2 <= g.t_eps;
-        if (!included || fully) return true;
-        float near2, far2;
-        tight_box_dist2(xp, w.cbmin + c, w.cbmax + c, g.ns, d, near2, far2);
-        if (near2 > g.t_extra || far2 <= g.t_eps) return true;
-        const int qb = __ldg(w.cell_start + c), qe = __ldg(w.cell_start + c + 1);
-        for (int q = qb; q < qe; q++) {
-            float d2 = 0.f;
-            for (int l = 0; l < d; l++) d2 = dist_step(xp[l], __ldg(w.X + (size_t)l * g.ns + q), d2);
-            if (!(d2 > g.t_eps && d2 <= g.t_extra)) continue;
-            pairs++;
-            bool resolved = true;
-            float acc = 0.f;
-            for (int l = 0; l < d; l++) {
-                const float lo = __ldg(w.qlo + (size_t)l * g.ns + q), hi = __ldg(w.qhi + (size_t)l * g.ns + q);
-                float m;
-                if (xp[l] >= hi) m = hi;
-                else if (xp[l] <= lo) m = lo;
-                else { resolved = false; break; }
-                acc = dist_step(m, xp[l], acc);
-            }
-            const bool in_eps = resolved ? (acc <= g.t_eps) : mbr_exact<D>(g, w, q, xp);
-            if (in_eps) {
-                violated = true;
-                *flag = 0;
-                return false;
-            }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+        float xp[DM];
+        int gp[DM];
+        int obase = 0;
+        for (int l = 0; l < d; l++) {
+            xp[l] = w.X[(size_t)l * g.ns + i];
+            gp[l] = cell_dim(xp[l], g);
+            if (l < g.od) obase += gp[l] * g.wpow[l];
         }
-        return true;
-    });
+        bool violated = false;
+        for_stencil_cells(g, w, 1, g.r_extra, gp, obase, d, [&](int c) {
+            if (*flag == 0) return false;
+            float sm2 = 0.f, lg2 = 0.f;
+            for (int l = 0; l < d; l++)
+                box_terms(xp[l], __ldg(w.cell_dims + (size_t)l * g.ns + c), g.side, sm2, lg2);
+            const bool included = sm2 <= g.t_extra;
+            const bool fully = lg2 <= g.t_eps;
+            if (!included || fully) return true;
+            float near2, far2;
+            tight_box_dist2(xp, w.cbmin + c, w.cbmax + c, g.ns, d, near2, far2);
+            if (near2 > g.t_extra || far2 <= g.t_eps) return true;
+            float lb2, ub2;
+            tight_box_dist2(xp, w.ulo + c, w.uhi + c, g.ns, d, lb2, ub2);
+            if (lb2 > g.t_eps) return true;  // no pair of this cell can have its MBR within eps
+            const int qb = __ldg(w.cell_start + c), qe = __ldg(w.cell_start + c + 1);
+            for (int q = qb; q < qe; q++) {
+                float d2 = 0.f;
+                for (int l = 0; l < d; l++) d2 = dist_step(xp[l], __ldg(w.X + (size_t)l * g.ns + q), d2);
+                if (!(d2 > g.t_eps && d2 <= g.t_extra)) continue;
+                pairs++;
+                bool resolved = true;
+                float acc = 0.f;
+                for (int l = 0; l < d; l++) {
+                    const float lo = __ldg(w.qlo + (size_t)l * g.ns + q), hi = __ldg(w.qhi + (size_t)l * g.ns + q);
+                    float m;
+                    if (xp[l] >= hi) m = hi;
+                    else if (xp[l] <= lo) m = lo;
+                    else { resolved = false; break; }
+                    acc = dist_step(m, xp[l], acc);
+                }
+                const bool in_eps = resolved ? (acc <= g.t_eps) : mbr_exact<D>(g, w, q, xp);
+                if (in_eps) {
+                    violated = true;
+                    *flag = 0;
+                    return false;
+                }
+            }
+            return true;
+        });
+        if (violated || *flag == 0) break;
+    }
     if (pairs) atomicAdd(w.ctrl + kCtrlPairs, pairs);
-    (void)violated;
 }
 
 #define EGG_DISPATCH_D(d, KERNEL, ...)                \
@@ -220,10 +245,14 @@ __global__ void __launch_bounds__(128) k_annulus(Geom g, Work w) {
         default: KERNEL<0> __VA_ARGS__; break;        \
     }
 
+// Both kernels return at once unless the update left the flag at 1; the
+// grids are bounded so that the common early exit costs little.
 void launch_extra_check(const Geom& g, const Work& w, cudaStream_t st) {
     const int threads = 128;
-    const int blocks = (g.n + threads - 1) / threads;
+    int blocks = (g.n + threads - 1) / threads;
+    if (blocks > 148 * 8) blocks = 148 * 8;
     EGG_DISPATCH_D(g.d, k_ball_bbox, <<<blocks, threads, 0, st>>>(g, w));
+    k_cell_ballbox<<<blocks, 256, 0, st>>>(g, w);
     EGG_DISPATCH_D(g.d, k_annulus, <<<blocks, threads, 0, st>>>(g, w));
 }
 

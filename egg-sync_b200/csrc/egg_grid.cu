@@ -420,21 +420,12 @@ __global__ void __launch_bounds__(256) k_cell_sums(Geom g, Work w) {
     (void)DM;
 }
 
-// Cells spanning more than one warp (the heavily populated ones): combine the
-// warp partials in FP64 in a fixed order, one warp per listed cell.  The list
-// order depends on scheduling, the result of every cell does not.
+// one big spanning cell, the whole warp: lanes stride over its warp partials
 template <int D>
-__global__ void __launch_bounds__(256) k_cell_sums_fix(Geom g, Work w) {
+__device__ void combine_big(const Geom& g, const Work& w, int c, int wh, int wt, int lane, int nw) {
     constexpr int DM = D > 0 ? D : 1;
     const int d = D > 0 ? D : g.d;
-    const int lane = threadIdx.x & 31;
-    const int count = w.ctrl[kCtrlSpanCount];
-    const int nw = (g.n + 31) >> 5;
-    const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < count; e += warps) {
-        const int c = w.span_list[e];
-        const int cs = w.cell_start[c], ce = w.cell_start[c + 1];
-        const int wh = cs >> 5, wt = (ce - 1) >> 5;
+    {
         if (D > 0) {
             // every dimension in one pass: 4*D independent loads per partial
             double S[DM], Mm[DM], mn[DM], mx[DM];
@@ -490,6 +481,54 @@ __global__ void __launch_bounds__(256) k_cell_sums_fix(Geom g, Work w) {
                     w.cbmax[(size_t)l * g.ns + c] = (float)mx;
                 }
             }
+        }
+    }
+}
+
+// Cells spanning more than one warp (the heavily populated ones): combine the
+// warp partials in FP64 in a fixed order, one warp per listed cell.  The list
+// order depends on scheduling, the result of every cell does not.
+template <int D>
+__global__ void __launch_bounds__(256) k_cell_sums_fix(Geom g, Work w) {
+    const int d = D > 0 ? D : g.d;
+    const int lane = threadIdx.x & 31;
+    const int count = w.ctrl[kCtrlSpanCount];
+    const int nw = (g.n + 31) >> 5;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int e0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; e0 < count; e0 += warps * 32) {
+        // lane = list entry.  Cells over at most three warps (nearly all: a
+        // small cell straddling a warp boundary) are summed by their lane;
+        // bigger ones by the whole warp below.
+        const int e = e0 + lane;
+        int c = 0, wh = 0, wt = -1;
+        if (e < count) {
+            c = w.span_list[e];
+            wh = w.cell_start[c] >> 5;
+            wt = (w.cell_start[c + 1] - 1) >> 5;
+        }
+        const bool big = e < count && wt - wh > 2;
+        if (e < count && !big) {
+            for (int l = 0; l < d; l++) {
+                double S = 0.0, Mm = 0.0, mn = 1e300, mx = -1e300;
+                for (int k = wh; k <= wt; k++) {
+                    const int rec = (k == wh) ? 1 : 0;
+                    S += w.wpart[wp_idx(0, l, d, rec, nw, k)];
+                    Mm += w.wpart[wp_idx(1, l, d, rec, nw, k)];
+                    mn = fmin(mn, w.wpart[wp_idx(2, l, d, rec, nw, k)]);
+                    mx = fmax(mx, w.wpart[wp_idx(3, l, d, rec, nw, k)]);
+                }
+                w.css[(size_t)l * g.ns + c] = (float)S;
+                w.csm[(size_t)l * g.ns + c] = (float)Mm;
+                w.cbmin[(size_t)l * g.ns + c] = (float)mn;
+                w.cbmax[(size_t)l * g.ns + c] = (float)mx;
+            }
+        }
+        unsigned todo = __ballot_sync(0xffffffffu, big);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            combine_big<D>(g, w, __shfl_sync(0xffffffffu, c, src), __shfl_sync(0xffffffffu, wh, src),
+                           __shfl_sync(0xffffffffu, wt, src), lane, nw);
         }
     }
 }

@@ -240,6 +240,8 @@ void prepare(Instance& I, const Geom& g, int max_iter) {
     add((void**)&w.md, 4 * d * ns);
     add((void**)&w.qlo, 4 * d * ns);
     add((void**)&w.qhi, 4 * d * ns);
+    add((void**)&w.ulo, 4 * d * ns);
+    add((void**)&w.uhi, 4 * d * ns);
     add((void**)&w.orig, 4 * ns);
     add((void**)&w.orig_tmp, 4 * ns);
     add((void**)&w.perm, 4 * ns);
@@ -598,7 +600,7 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
         // launches: reset + transpose, per iteration (begin, build, 2 cell
         // sums, update, mark, 2 extra, end), final build + labels
         const int build_l = 3 * I.plan.count + 6;
-        stats->launches = 2 + iters * (build_l + 9) + build_l + 1;
+        stats->launches = 2 + iters * (build_l + 10) + build_l + 1;
     }
     if (I.h_ctrl[kCtrlStatus] & ~kErrNonFinite)
         throw ArgError{EGG_ERR_INTERNAL, "kernel consistency check failed (status bits " +
