@@ -101,7 +101,8 @@ struct Work {
     unsigned char* dirty[2];   // [n_outer]
     unsigned char* need;       // [n_outer]
     unsigned char* viol_orig;  // [ns] by original index
-    int* span_list;            // [ns/32 + 1] cells whose points span several warps
+    int* span_list;            // [ns/32 + 1] cells whose points span 2-3 warps
+    int* big_list;             // [ns/128 + 1] cells whose points span 4 or more warps
 };
 
 enum : int {
@@ -120,7 +121,9 @@ enum : int {
     kCtrlForce = 12,      // recompute every point (first iteration of a run)
     kCtrlComputed = 13,   // points recomputed by the update (statistics)
     kCtrlFullUpdate = 14, // recompute every point in every iteration
-    kCtrlSpanCount = 15,  // cells listed in span_list by the cell-sums kernel
+    kCtrlSpanCount = 15,  // cells over 2-3 warps listed in span_list by the cell-sums kernel
+    kCtrlBigCount = 16,   // cells over 4 or more warps listed in big_list
+    kCtrlWords = 32,      // size of the control-word array
 };
 
 // ------------------------------------------------------------------------

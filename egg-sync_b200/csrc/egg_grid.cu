@@ -116,6 +116,7 @@ __global__ void __launch_bounds__(256) k_check_cells(Geom g, Work w) {
 __global__ void k_build_begin(int* ctrl) {
     ctrl[kCtrlChanged] = 0;
     ctrl[kCtrlSpanCount] = 0;
+    ctrl[kCtrlBigCount] = 0;
 }
 
 #define EGG_SKIP_IF_UNCHANGED(ctrl) \
@@ -358,7 +359,10 @@ __global__ void __launch_bounds__(256) k_cell_sums(Geom g, Work w) {
     const bool complete = seg_end && cs >= wb && ce <= wb + 32;
     // a cell that starts in this warp and continues past it: list it once
     // for the FP64 combination of its warp partials
-    if (seg_end && cs >= wb && ce > wb + 32) w.span_list[atomicAdd(w.ctrl + kCtrlSpanCount, 1)] = c;
+    if (seg_end && cs >= wb && ce > wb + 32) {
+        if (((ce - 1) >> 5) - (cs >> 5) > 2) w.big_list[atomicAdd(w.ctrl + kCtrlBigCount, 1)] = c;
+        else w.span_list[atomicAdd(w.ctrl + kCtrlSpanCount, 1)] = c;
+    }
     for (int l = 0; l < d; l++) {
         float s = 0.f, m = 0.f, x = 0.f;
         if (valid) {
@@ -485,50 +489,39 @@ __device__ void combine_big(const Geom& g, const Work& w, int c, int wh, int wt,
     }
 }
 
-// Cells spanning more than one warp (the heavily populated ones): combine the
-// warp partials in FP64 in a fixed order, one warp per listed cell.  The list
-// order depends on scheduling, the result of every cell does not.
+// Cells spanning more than one warp: combine the warp partials in FP64 in a
+// fixed order.  Cells over four or more warps (the heavily populated ones)
+// get a warp each; the others (nearly all: a small cell straddling a warp
+// boundary) a thread each.  The list order depends on scheduling, the result
+// of every cell does not.
 template <int D>
 __global__ void __launch_bounds__(256) k_cell_sums_fix(Geom g, Work w) {
     const int d = D > 0 ? D : g.d;
     const int lane = threadIdx.x & 31;
-    const int count = w.ctrl[kCtrlSpanCount];
     const int nw = (g.n + 31) >> 5;
+    const int big = w.ctrl[kCtrlBigCount];
     const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int e0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; e0 < count; e0 += warps * 32) {
-        // lane = list entry.  Cells over at most three warps (nearly all: a
-        // small cell straddling a warp boundary) are summed by their lane;
-        // bigger ones by the whole warp below.
-        const int e = e0 + lane;
-        int c = 0, wh = 0, wt = -1;
-        if (e < count) {
-            c = w.span_list[e];
-            wh = w.cell_start[c] >> 5;
-            wt = (w.cell_start[c + 1] - 1) >> 5;
-        }
-        const bool big = e < count && wt - wh > 2;
-        if (e < count && !big) {
-            for (int l = 0; l < d; l++) {
-                double S = 0.0, Mm = 0.0, mn = 1e300, mx = -1e300;
-                for (int k = wh; k <= wt; k++) {
-                    const int rec = (k == wh) ? 1 : 0;
-                    S += w.wpart[wp_idx(0, l, d, rec, nw, k)];
-                    Mm += w.wpart[wp_idx(1, l, d, rec, nw, k)];
-                    mn = fmin(mn, w.wpart[wp_idx(2, l, d, rec, nw, k)]);
-                    mx = fmax(mx, w.wpart[wp_idx(3, l, d, rec, nw, k)]);
-                }
-                w.css[(size_t)l * g.ns + c] = (float)S;
-                w.csm[(size_t)l * g.ns + c] = (float)Mm;
-                w.cbmin[(size_t)l * g.ns + c] = (float)mn;
-                w.cbmax[(size_t)l * g.ns + c] = (float)mx;
+    for (int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < big; e += warps) {
+        const int c = w.big_list[e];
+        combine_big<D>(g, w, c, w.cell_start[c] >> 5, (w.cell_start[c + 1] - 1) >> 5, lane, nw);
+    }
+    const int count = w.ctrl[kCtrlSpanCount];
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {
+        const int c = w.span_list[e];
+        const int wh = w.cell_start[c] >> 5, wt = (w.cell_start[c + 1] - 1) >> 5;
+        for (int l = 0; l < d; l++) {
+            double S = 0.0, Mm = 0.0, mn = 1e300, mx = -1e300;
+            for (int k = wh; k <= wt; k++) {
+                const int rec = (k == wh) ? 1 : 0;
+                S += w.wpart[wp_idx(0, l, d, rec, nw, k)];
+                Mm += w.wpart[wp_idx(1, l, d, rec, nw, k)];
+                mn = fmin(mn, w.wpart[wp_idx(2, l, d, rec, nw, k)]);
+                mx = fmax(mx, w.wpart[wp_idx(3, l, d, rec, nw, k)]);
             }
-        }
-        unsigned todo = __ballot_sync(0xffffffffu, big);
-        while (todo) {
-            const int src = __ffs(todo) - 1;
-            todo &= todo - 1;
-            combine_big<D>(g, w, __shfl_sync(0xffffffffu, c, src), __shfl_sync(0xffffffffu, wh, src),
-                           __shfl_sync(0xffffffffu, wt, src), lane, nw);
+            w.css[(size_t)l * g.ns + c] = (float)S;
+            w.csm[(size_t)l * g.ns + c] = (float)Mm;
+            w.cbmin[(size_t)l * g.ns + c] = (float)mn;
+            w.cbmax[(size_t)l * g.ns + c] = (float)mx;
         }
     }
 }

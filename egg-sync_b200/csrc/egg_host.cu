@@ -209,7 +209,7 @@ Instance& instance() {
     I->dev = dev;
     EGG_CHECK(cudaStreamCreateWithFlags(&I->st, cudaStreamNonBlocking));
     for (auto& e2 : I->ev) EGG_CHECK(cudaEventCreate(&e2));
-    EGG_CHECK(cudaMallocHost((void**)&I->h_ctrl, 16 * sizeof(int)));
+    EGG_CHECK(cudaMallocHost((void**)&I->h_ctrl, kCtrlWords * sizeof(int)));
     g_inst[dev] = I;
     return *I;
 }
@@ -263,7 +263,7 @@ void prepare(Instance& I, const Geom& g, int max_iter) {
     add((void**)&w.st_delta, 4 * 3 * (size_t)st_cap);
     add((void**)&w.st_off, 3 * (size_t)st_cap * odp);
     add((void**)&w.table, 4 * 3 * (size_t)TW);
-    add((void**)&w.ctrl, 4 * 16);
+    add((void**)&w.ctrl, 4 * kCtrlWords);
     add((void**)&w.stamps, 8 * 4 * ((size_t)max_iter + 2));
     add((void**)&w.labels, 4 * ns);
     add((void**)&w.iter_flags, 4 * ((size_t)max_iter + 2));
@@ -273,6 +273,7 @@ void prepare(Instance& I, const Geom& g, int max_iter) {
     add((void**)&w.need, (size_t)g.n_outer + 1);
     add((void**)&w.viol_orig, ns);
     add((void**)&w.span_list, 4 * ((size_t)nw + 1));
+    add((void**)&w.big_list, 4 * ((size_t)nw / 4 + 1));
     for (auto& p : plan) off += align_up(p.second);
     if (off > I.cap) {
         destroy_graph(I);
@@ -328,7 +329,7 @@ void prepare(Instance& I, const Geom& g, int max_iter) {
 // loop control kernels
 // ------------------------------------------------------------------------
 __global__ void k_ctrl_reset(Work w, int max_iter, int full_update) {
-    if (threadIdx.x < 16) w.ctrl[threadIdx.x] = 0;
+    for (int t = threadIdx.x; t < kCtrlWords; t += blockDim.x) w.ctrl[t] = 0;
     __syncwarp();
     if (threadIdx.x == 0) {
         w.ctrl[kCtrlMaxIter] = max_iter;
@@ -456,7 +457,7 @@ void load_input(Instance& I, const float* x, int full_update = 0) {
 }
 
 void check_status_bits(Instance& I) {
-    EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, 16 * sizeof(int), cudaMemcpyDeviceToHost, I.st));
+    EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, kCtrlWords * sizeof(int), cudaMemcpyDeviceToHost, I.st));
     EGG_CHECK(cudaStreamSynchronize(I.st));
     if (I.h_ctrl[kCtrlStatus] & kErrNonFinite) throw ArgError{EGG_ERR_INPUT, "input holds NaN or Inf"};
 }
@@ -526,7 +527,7 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
             for (auto& e : I.prof) EGG_CHECK(cudaEventCreate(&e));
         for (;;) {
             enqueue_iteration(I, 0, 0, prof);
-            EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, 16 * sizeof(int), cudaMemcpyDeviceToHost, I.st));
+            EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, kCtrlWords * sizeof(int), cudaMemcpyDeviceToHost, I.st));
             EGG_CHECK(cudaStreamSynchronize(I.st));
             if (prof) {
                 for (int k = 0; k < 4; k++) {
@@ -555,7 +556,7 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
     }
     EGG_CHECK(cudaEventRecord(I.ev[3], I.st));
     if (!dev_out) EGG_CHECK(cudaMemcpyAsync(labels, lab, sizeof(int) * (size_t)g.n, cudaMemcpyDeviceToHost, I.st));
-    EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, 16 * sizeof(int), cudaMemcpyDeviceToHost, I.st));
+    EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, kCtrlWords * sizeof(int), cudaMemcpyDeviceToHost, I.st));
     EGG_CHECK(cudaEventRecord(I.ev[4], I.st));
     EGG_CHECK(cudaStreamSynchronize(I.st));
     EGG_CHECK(cudaGetLastError());
@@ -624,11 +625,11 @@ int step(const float* x, int64_t n, int32_t d, float eps, float* x_next, int32_t
     launch_need(I.g, I.w, st);
     int* cnt_sorted = I.w.orig_tmp;  // free once the grid is built
     launch_update(I.g, I.w, cnt_sorted, st);
-    EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, 16 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, kCtrlWords * sizeof(int), cudaMemcpyDeviceToHost, st));
     EGG_CHECK(cudaStreamSynchronize(st));
     flags[0] = I.h_ctrl[kCtrlFlag];
     launch_extra_check(I.g, I.w, st);
-    EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, 16 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, kCtrlWords * sizeof(int), cudaMemcpyDeviceToHost, st));
     // updated positions back to the original order (staged in qlo, free now)
     const bool dev_x = is_device_ptr(x_next);
     float* xo = dev_x ? x_next : I.xin;
@@ -658,7 +659,7 @@ int grid(const float* x, int64_t n, int32_t d, float eps, int32_t* order, int32_
     load_input(I, x);
     check_status_bits(I);
     launch_build(I.g, I.w, I.plan, I.st);
-    EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, 16 * sizeof(int), cudaMemcpyDeviceToHost, I.st));
+    EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, kCtrlWords * sizeof(int), cudaMemcpyDeviceToHost, I.st));
     EGG_CHECK(cudaStreamSynchronize(I.st));
     const int M = I.h_ctrl[kCtrlM];
     auto out = [&](int32_t* dst, const int* src, size_t cnt) {
