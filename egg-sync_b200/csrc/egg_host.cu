@@ -674,6 +674,112 @@ int grid(const float* x, int64_t n, int32_t d, float eps, int32_t* order, int32_
     return EGG_OK;
 }
 
+// ------------------------------------------------------------------------
+// Grid build without any device allocation.
+//
+// Some callers cannot allocate device memory: a host framework that has
+// reserved the device through its own memory pool (cudaMalloc then fails or
+// escapes the framework's accounting), or a latency-critical caller for
+// which the implicit device synchronisation of cudaMalloc/cudaFree is not
+// acceptable.  egg_sync_grid_noalloc serves them: it runs the same grid
+// build as egg_sync_grid, with every scratch buffer carved out of one
+// statically sized device array that belongs to this library.
+// ------------------------------------------------------------------------
+namespace {
+
+constexpr int kNoAllocMaxN = 65536;
+constexpr int kNoAllocMaxD = 4;
+constexpr size_t kNoAllocBytes = (size_t)8 << 20;  // 8 MiB
+
+// Every GPU on which libeggsync.so is loaded holds this array until the
+// process exits.  In host code its name is only a stand-in: the device
+// address comes from cudaGetSymbolAddress.
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Device address of g_noalloc_scratch for each device, looked up on the first
+// call on that device (with that device current).
+void* g_noalloc_addr[256] = {};
+
+__global__ void k_noalloc_reset(int* ctrl) {
+    for (int t = threadIdx.x; t < kCtrlWords; t += blockDim.x) ctrl[t] = 0;
+}
+
+}  // namespace
+
+int grid_noalloc(const float* x, int64_t n, int32_t d, float eps, int32_t* order, int32_t* cell_of,
+                 int32_t* cell_start, int32_t* n_cells, void* stream) {
+    if (!x || !order || !cell_of || !cell_start || !n_cells) throw ArgError{EGG_ERR_ARG, "NULL argument"};
+    if (n < 1 || n > kNoAllocMaxN || d < 1 || d > kNoAllocMaxD)
+        throw ArgError{EGG_ERR_ARG, "egg_sync_grid_noalloc supports 1 <= n <= 65536 and 1 <= d <= 4 (got n = " +
+                                        std::to_string(n) + ", d = " + std::to_string(d) + ")"};
+    const Geom g = make_geom(n, d, eps);
+    int dev = 0;
+    EGG_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) throw ArgError{EGG_ERR_INTERNAL, "device ordinal out of range"};
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        EGG_CHECK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_addr[dev] = p;
+    }
+
+    // carve the grid build's buffers out of the static array
+    const size_t ns = (size_t)g.ns;
+    const int tiles = (g.n + kSortTile - 1) / kSortTile;
+    const int nb = (g.n + kHeadsBlock - 1) / kHeadsBlock;
+    Work w;
+    memset(&w, 0, sizeof(w));
+    float* xin = nullptr;
+    char* base = (char*)g_noalloc_addr[dev];
+    size_t off = 0;
+    auto take = [&](void** ptr, size_t bytes) {
+        *ptr = base + off;
+        off += align_up(bytes);
+    };
+    take((void**)&w.X, 4 * d * ns);
+    take((void**)&w.Xn, 4 * d * ns);
+    take((void**)&w.orig, 4 * ns);
+    take((void**)&w.orig_tmp, 4 * ns);
+    take((void**)&w.perm, 4 * ns);
+    take((void**)&w.perm_tmp, 4 * ns);
+    take((void**)&w.cell_of, 4 * ns);
+    take((void**)&w.cell_start, 4 * (ns + 1));
+    take((void**)&w.cell_dims, 4 * d * ns);
+    take((void**)&w.cell_outer, 4 * ns);
+    take((void**)&w.outer_begin, 4 * ((size_t)g.n_outer + 1));
+    take((void**)&w.hist, 4 * 256 * (size_t)tiles);
+    take((void**)&w.digit_total, 4 * 256);
+    take((void**)&w.block_sums, 4 * (size_t)nb);
+    take((void**)&w.ctrl, 4 * kCtrlWords);
+    take((void**)&w.need, (size_t)g.n_outer + 1);
+    take((void**)&xin, 4 * (size_t)g.n * d);
+    if (off > kNoAllocBytes) throw ArgError{EGG_ERR_INTERNAL, "static scratch too small for this geometry"};
+
+    cudaStream_t st = (cudaStream_t)stream;
+    const SortPlan plan = make_plan(g);
+    // the array keeps the previous call's contents: the control words must
+    // start at zero (every other buffer is fully written before it is read)
+    k_noalloc_reset<<<1, 32, 0, st>>>(w.ctrl);
+    const float* src = x;
+    if (!is_device_ptr(x)) {
+        EGG_CHECK(cudaMemcpyAsync(xin, x, sizeof(float) * (size_t)g.n * d, cudaMemcpyHostToDevice, st));
+        src = xin;
+    }
+    launch_transpose_in(g, w, src, st);
+    launch_build(g, w, plan, st);
+    int ctrl_h[kCtrlWords];
+    EGG_CHECK(cudaMemcpyAsync(ctrl_h, w.ctrl, sizeof(ctrl_h), cudaMemcpyDeviceToHost, st));
+    EGG_CHECK(cudaStreamSynchronize(st));
+    if (ctrl_h[kCtrlStatus] & kErrNonFinite) throw ArgError{EGG_ERR_INPUT, "input holds NaN or Inf"};
+    const int M = ctrl_h[kCtrlM];
+    EGG_CHECK(cudaMemcpyAsync(order, w.orig, sizeof(int) * (size_t)g.n, cudaMemcpyDefault, st));
+    EGG_CHECK(cudaMemcpyAsync(cell_of, w.cell_of, sizeof(int) * (size_t)g.n, cudaMemcpyDefault, st));
+    EGG_CHECK(cudaMemcpyAsync(cell_start, w.cell_start, sizeof(int) * ((size_t)M + 1), cudaMemcpyDefault, st));
+    EGG_CHECK(cudaStreamSynchronize(st));
+    EGG_CHECK(cudaGetLastError());
+    *n_cells = M;
+    return EGG_OK;
+}
+
 int release() {
     for (auto& kv : g_inst) {
         Instance* I = kv.second;
@@ -723,6 +829,14 @@ __attribute__((visibility("default"))) int egg_sync_grid(const float* x, int64_t
                                                          int32_t* order, int32_t* cell_of, int32_t* cell_start,
                                                          int32_t* n_cells, void* stream) {
     return egg::guarded([&] { return egg::grid(x, n, d, eps, order, cell_of, cell_start, n_cells, stream); });
+}
+
+__attribute__((visibility("default"))) int egg_sync_grid_noalloc(const float* x, int64_t n, int32_t d, float eps,
+                                                                 int32_t* order, int32_t* cell_of,
+                                                                 int32_t* cell_start, int32_t* n_cells,
+                                                                 void* stream) {
+    return egg::guarded(
+        [&] { return egg::grid_noalloc(x, n, d, eps, order, cell_of, cell_start, n_cells, stream); });
 }
 
 __attribute__((visibility("default"))) const char* egg_status_str(int s) {

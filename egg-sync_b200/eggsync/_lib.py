@@ -22,8 +22,8 @@ EGG_ERR_NO_DEVICE = -5
 EGG_ERR_INTERNAL = -6
 
 # every symbol include/eggsync.h declares
-EXPORTS = ("egg_opts_default", "egg_sync_run", "egg_sync_step", "egg_sync_grid", "egg_status_str",
-           "egg_last_error", "egg_release", "egg_abi_version")
+EXPORTS = ("egg_opts_default", "egg_sync_run", "egg_sync_step", "egg_sync_grid", "egg_sync_grid_noalloc",
+           "egg_status_str", "egg_last_error", "egg_release", "egg_abi_version")
 
 
 class EggOpts(C.Structure):
@@ -75,6 +75,8 @@ def load():
     L.egg_sync_step.restype = C.c_int
     L.egg_sync_grid.argtypes = [vp, C.c_int64, C.c_int32, C.c_float, vp, vp, vp, C.POINTER(C.c_int32), vp]
     L.egg_sync_grid.restype = C.c_int
+    L.egg_sync_grid_noalloc.argtypes = [vp, C.c_int64, C.c_int32, C.c_float, vp, vp, vp, C.POINTER(C.c_int32), vp]
+    L.egg_sync_grid_noalloc.restype = C.c_int
     L.egg_status_str.argtypes = [C.c_int]
     L.egg_status_str.restype = C.c_char_p
     L.egg_last_error.argtypes = []

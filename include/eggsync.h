@@ -100,6 +100,27 @@ int egg_sync_step(const float *x, int64_t n, int32_t d, float eps, float *x_next
 int egg_sync_grid(const float *x, int64_t n, int32_t d, float eps, int32_t *order, int32_t *cell_of,
                   int32_t *cell_start, int32_t *n_cells, void *stream);
 
+/* The grid build of egg_sync_grid, for callers that must not allocate device
+ * memory.  No counterpart in the reference.  Callers whose device memory is
+ * owned by their own pool (a framework that has reserved the device, where
+ * cudaMalloc fails or escapes its accounting) or that cannot afford the
+ * device synchronisation cudaMalloc/cudaFree imply can use this entry point:
+ * it calls no cudaMalloc, cudaFree or allocating library routine.  All of its
+ * scratch lives in one file-scope device array of 8 MiB that every GPU which
+ * loads the library holds until the process exits; inputs and outputs are
+ * still the caller's (host or device pointers).
+ * Limits: 1 <= n <= 65536 and 1 <= d <= 4; larger inputs return EGG_ERR_ARG.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  Every call reuses the same array and finds the
+ * previous call's contents in it (the call clears what must start at zero);
+ * two calls overlapping on the GPU would race on it.  Calls through this
+ * library are serialised and each one has finished on the GPU before it
+ * returns.  stream: the cudaStream_t the work runs on (NULL = legacy default
+ * stream).  Outputs as for egg_sync_grid. */
+int egg_sync_grid_noalloc(const float *x, int64_t n, int32_t d, float eps, int32_t *order, int32_t *cell_of,
+                          int32_t *cell_start, int32_t *n_cells, void *stream);
+
 /* Human-readable name of a status value. */
 const char *egg_status_str(int status);
 
