@@ -48,6 +48,9 @@ struct Geom {
     float t_extra;     // ... <= eps_extra
     int sub_dims;      // dimensions in the within-cell (sub-cell) sort key
     int sub_bits;      // bits per dimension of the sub-cell key (sub_dims*sub_bits <= 8)
+    int stop_rule;     // 0 = the reference's convergence flag, 1 = order parameter >= lam
+    int order_mode;    // 0 = no order parameter, 1 = final only, 2 = every iteration
+    float lam;         // order-parameter threshold of stop rule 1
     int wpow[32];      // width^l for l < od
 };
 
@@ -103,6 +106,12 @@ struct Work {
     unsigned char* viol_orig;  // [ns] by original index
     int* span_list;            // [ns/32 + 1] cells whose points span 2-3 warps
     int* big_list;             // [ns/128 + 1] cells whose points span 4 or more warps
+    // local order parameter (FP64): per-block partials, per-iteration [lo, hi]
+    double* rpart;             // [2 * blocks]
+    double* rvals;             // [2 * (max_iter + 2)]; slot max_iter + 1 = final value
+    // union-find labelling
+    int* uf_parent;            // [ns]
+    int* uf_size;              // [ns]
 };
 
 enum : int {
@@ -123,6 +132,7 @@ enum : int {
     kCtrlFullUpdate = 14, // recompute every point in every iteration
     kCtrlSpanCount = 15,  // cells over 2-3 warps listed in span_list by the cell-sums kernel
     kCtrlBigCount = 16,   // cells over 4 or more warps listed in big_list
+    kCtrlLamReached = 17, // the order parameter's lower bound reached lambda this iteration
     kCtrlWords = 32,      // size of the control-word array
 };
 

@@ -274,6 +274,10 @@ void prepare(Instance& I, const Geom& g, int max_iter) {
     add((void**)&w.viol_orig, ns);
     add((void**)&w.span_list, 4 * ((size_t)nw + 1));
     add((void**)&w.big_list, 4 * ((size_t)nw / 4 + 1));
+    add((void**)&w.rpart, 8 * 2 * (size_t)((g.n + 127) / 128));
+    add((void**)&w.rvals, 8 * 2 * ((size_t)max_iter + 2));
+    add((void**)&w.uf_parent, 4 * ns);
+    add((void**)&w.uf_size, 4 * ns);
     for (auto& p : plan) off += align_up(p.second);
     if (off > I.cap) {
         destroy_graph(I);
@@ -344,7 +348,7 @@ __global__ void k_iter_begin(Work w) {
     w.stamps[4 * it + 0] = globaltimer();
 }
 
-__global__ void k_iter_end(Work w, cudaGraphConditionalHandle h, int in_graph) {
+__global__ void k_iter_end(Work w, cudaGraphConditionalHandle h, int in_graph, int stop_rule) {
     const int it = w.ctrl[kCtrlIter];
     const int flag = w.ctrl[kCtrlFlag];
     w.iter_flags[it] = flag;
@@ -352,7 +356,10 @@ __global__ void k_iter_end(Work w, cudaGraphConditionalHandle h, int in_graph) {
     const int next = it + 1;
     w.ctrl[kCtrlIter] = next;
     w.ctrl[kCtrlForce] = w.ctrl[kCtrlFullUpdate];
-    const int done = flag != 0 || next >= w.ctrl[kCtrlMaxIter];
+    // stop rule 0: the reference's flag (EGG_SynC.cu:1322); 1: the order
+    // parameter's certified lower bound reached lambda (SynC.cpp:277 semantics)
+    const int stop = stop_rule ? w.ctrl[kCtrlLamReached] : flag;
+    const int done = stop != 0 || next >= w.ctrl[kCtrlMaxIter];
     w.ctrl[kCtrlDone] = done;
     if (in_graph && done) cudaGraphSetConditional(h, 0);
 }
@@ -377,6 +384,7 @@ void enqueue_iteration(Instance& I, cudaGraphConditionalHandle h, int in_graph, 
     mark(2);
     launch_cell_sums(I.g, I.w, st);
     launch_need(I.g, I.w, st);
+    if (I.g.order_mode == 2 || I.g.stop_rule == 1) launch_order_param(I.g, I.w, -1, st);
     mark(3);
     mark(4);
     launch_update(I.g, I.w, nullptr, st);
@@ -385,7 +393,7 @@ void enqueue_iteration(Instance& I, cudaGraphConditionalHandle h, int in_graph, 
     mark(6);
     launch_extra_check(I.g, I.w, st);
     mark(7);
-    k_iter_end<<<1, 1, 0, st>>>(I.w, h, in_graph);
+    k_iter_end<<<1, 1, 0, st>>>(I.w, h, in_graph, I.g.stop_rule);
 }
 
 std::vector<char> graph_key(const Instance& I) {
@@ -505,9 +513,13 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
     if (opts_in) opts = *opts_in;
     int max_iter = opts.max_iter > 0 ? opts.max_iter : 1000;
     if (max_iter > 1000000) throw ArgError{EGG_ERR_ARG, "max_iter too large"};
-    if (opts.stop_rule != 0) throw ArgError{EGG_ERR_ARG, "stop_rule 1 (order parameter) is not available in this build"};
-    (void)lam;
+    if (opts.stop_rule < 0 || opts.stop_rule > 1) throw ArgError{EGG_ERR_ARG, "stop_rule must be 0 or 1"};
+    if (opts.order_param < 0 || opts.order_param > 2) throw ArgError{EGG_ERR_ARG, "order_param must be 0, 1 or 2"};
+    if (opts.stop_rule == 1 && !(lam > 0.0f && lam <= 1.0f)) throw ArgError{EGG_ERR_ARG, "lam must be in (0, 1]"};
     Geom g = make_geom(n, d, eps);
+    g.stop_rule = opts.stop_rule;
+    g.order_mode = opts.stop_rule == 1 ? 2 : opts.order_param;
+    g.lam = lam;
     Instance& I = instance();
     EGG_CHECK(cudaEventRecord(I.ev[0], I.st));
     order_after(I, stream);
@@ -545,7 +557,13 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
     launch_build(I.g, I.w, I.plan, I.st);
     const bool dev_out = is_device_ptr(labels);
     int* lab = dev_out ? labels : I.w.labels;
-    launch_labels(I.g, I.w, lab, I.st);
+    if (opts.labels_mode == 1) launch_labels(I.g, I.w, lab, I.st);
+    else launch_labels_uf(I.g, I.w, lab, I.st);
+    if (g.order_mode == 1) {
+        // the final positions' order parameter needs their cell sums
+        launch_cell_sums(I.g, I.w, I.st);
+        launch_order_param(I.g, I.w, max_iter + 1, I.st);
+    }
     if (opts.positions_out) {
         const bool dev_p = is_device_ptr(opts.positions_out);
         float* po = dev_p ? opts.positions_out : I.xin;
@@ -562,7 +580,7 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
     EGG_CHECK(cudaGetLastError());
 
     const int iters = I.h_ctrl[kCtrlIter];
-    const int converged = I.h_ctrl[kCtrlFlag] != 0;
+    const int converged = (g.stop_rule ? I.h_ctrl[kCtrlLamReached] : I.h_ctrl[kCtrlFlag]) != 0;
     if (stats) {
         const int M = I.h_ctrl[kCtrlM];
         stats->iterations = iters;
@@ -572,6 +590,20 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
         stats->status_bits = I.h_ctrl[kCtrlStatus];
         stats->workspace_bytes = (int64_t)I.used;
         stats->order_param = -1.0;
+        stats->order_param_lo = stats->order_param_hi = -1.0;
+        if (g.order_mode != 0) {
+            const int slot = g.order_mode == 1 ? max_iter + 1 : iters - 1;
+            double r[2];
+            EGG_CHECK(cudaMemcpy(r, I.w.rvals + 2 * slot, sizeof(r), cudaMemcpyDeviceToHost));
+            stats->order_param_lo = r[0];
+            stats->order_param_hi = r[1];
+            stats->order_param = 0.5 * (r[0] + r[1]);
+            if (g.order_mode == 2 && stats->itr_order_param) {
+                const int cnt = std::min(iters, stats->itr_cap);
+                EGG_CHECK(cudaMemcpy(stats->itr_order_param, I.w.rvals, sizeof(double) * 2 * (size_t)cnt,
+                                     cudaMemcpyDeviceToHost));
+            }
+        }
         stats->n_clusters = I.h_ctrl[kCtrlClusters];
         EGG_CHECK(cudaMemcpy(I.h_stamps, I.w.stamps, 8 * 4 * (size_t)iters, cudaMemcpyDeviceToHost));
         double st1 = 0, st2 = 0, st3 = 0;
@@ -600,8 +632,15 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
         }
         // launches: reset + transpose, per iteration (begin, build, 2 cell
         // sums, update, mark, 2 extra, end), final build + labels
+        // reset + transpose; per iteration: begin, build, 2 cell sums, need,
+        // [2 order parameter], update, mark, 3 extra check, end; then the
+        // final build, labels (1 or 4 kernels), [2 cell sums + 2 order
+        // parameter], [positions]
         const int build_l = 3 * I.plan.count + 6;
-        stats->launches = 2 + iters * (build_l + 10) + build_l + 1;
+        const int per_iter = build_l + 10 + ((g.order_mode == 2 || g.stop_rule == 1) ? 2 : 0);
+        const int final_l = build_l + (opts.labels_mode == 1 ? 1 : 4) + (g.order_mode == 1 ? 4 : 0) +
+                            (opts.positions_out ? 1 : 0);
+        stats->launches = 2 + iters * per_iter + final_l;
     }
     if (I.h_ctrl[kCtrlStatus] & ~kErrNonFinite)
         throw ArgError{EGG_ERR_INTERNAL, "kernel consistency check failed (status bits " +

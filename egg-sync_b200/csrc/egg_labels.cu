@@ -1,0 +1,90 @@
+// egg_labels.cu -- cluster extraction by GPU union-find.
+//
+// The reference labels a point with the compacted index of its final cell
+// when that cell holds more than one point, else -1
+// (src/algorithms/EGG_SynC.cu:1205-1227, 1504-1522).  Here the collapsed
+// points are joined into components by a lock-free union-find: every pair of
+// consecutive cell-sorted points in the same final cell is an edge; a link
+// hooks the larger root onto the smaller one with atomicCAS, so every
+// component's root is its smallest sorted index, i.e. the first point of the
+// cell, whatever the order of the atomics.  After full path compression a
+// point's label is the cell index of its root when the component holds more
+// than one point: the reference's partition and label values, deterministic.
+#include "egg_common.cuh"
+#include "egg_kernels.h"
+
+namespace egg {
+
+namespace {
+
+__device__ __forceinline__ int uf_find(int* parent, int x) {
+    int p = parent[x];
+    while (p != x) {
+        const int gp = parent[p];
+        if (gp != p) parent[x] = gp;  // path halving; any order of these writes is safe
+        x = p;
+        p = gp;
+    }
+    return x;
+}
+
+__device__ __forceinline__ void uf_union(int* parent, int a, int b) {
+    for (;;) {
+        a = uf_find(parent, a);
+        b = uf_find(parent, b);
+        if (a == b) return;
+        if (a < b) {
+            const int t = a;
+            a = b;
+            b = t;
+        }
+        // hook root a (larger) below root b; retry if a stopped being a root
+        if (atomicCAS(parent + a, a, b) == a) return;
+    }
+}
+
+}  // namespace
+
+__global__ void k_uf_init(Geom g, int* __restrict__ parent, int* __restrict__ csize) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+        parent[i] = i;
+        csize[i] = 0;
+    }
+}
+
+// edge (i, i+1) whenever both points lie in the same final cell
+__global__ void k_uf_link(Geom g, Work w, int* parent) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i + 1 < g.n; i += gridDim.x * blockDim.x)
+        if (w.cell_of[i] == w.cell_of[i + 1]) uf_union(parent, i, i + 1);
+}
+
+__global__ void k_uf_compress(Geom g, int* parent, int* csize) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+        const int r = uf_find(parent, i);
+        atomicAdd(csize + r, 1);
+    }
+}
+
+__global__ void k_uf_labels(Geom g, Work w, const int* __restrict__ parent, const int* __restrict__ csize,
+                            int* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+        // parent[i] may still point to a non-root after compress (halving),
+        // so follow it to the root without writing
+        int r = parent[i];
+        while (parent[r] != r) r = parent[r];
+        const bool multi = csize[r] > 1;
+        out[w.orig[i]] = multi ? w.cell_of[r] : -1;
+        if (multi && r == i) atomicAdd(w.ctrl + kCtrlClusters, 1);
+    }
+}
+
+void launch_labels_uf(const Geom& g, const Work& w, int* out, cudaStream_t st) {
+    int blocks = (g.n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_uf_init<<<blocks, 256, 0, st>>>(g, w.uf_parent, w.uf_size);
+    k_uf_link<<<blocks, 256, 0, st>>>(g, w, w.uf_parent);
+    k_uf_compress<<<blocks, 256, 0, st>>>(g, w.uf_parent, w.uf_size);
+    k_uf_labels<<<blocks, 256, 0, st>>>(g, w, w.uf_parent, w.uf_size, out);
+}
+
+}  // namespace egg

@@ -1,0 +1,86 @@
+// egg_stencil.cuh -- candidate-cell enumeration shared by the per-point kernels.
+//
+// For a point with cell dims gi (outer id obase) the candidate cells are the
+// inner cells of the outer cells in the box stencil [-r, r]^od (the
+// reference's pre-grid, EGG_SynC.cu:386-536), restricted in dimension od to
+// [gi_od - r - 1, gi_od + r + 1]: cells beyond fail the reference's box test
+// in exact and rounded arithmetic alike (their gap exceeds (r+1)*side > eps).
+//
+// Must be called by all 32 lanes of a warp.  When every lane has the same
+// outer cell, the warp resolves the stencil entries in parallel (lane =
+// entry) and visits each candidate cell with all lanes in lockstep (the cell
+// records become broadcast loads); otherwise each lane walks its own stencil.
+// fn(c) is called once per candidate cell per lane, in increasing stencil
+// entry then increasing cell order in both paths.
+#pragma once
+
+#include "egg_common.cuh"
+
+namespace egg {
+
+template <typename F>
+__device__ __forceinline__ void for_candidates(const Geom& g, const Work& w, const int* gi, int obase, int lane,
+                                               int d, F&& fn) {
+    const int nst = w.st_count[0];
+    const int ob0 = __shfl_sync(0xffffffffu, obase, 0);
+    if (__all_sync(0xffffffffu, obase == ob0)) {
+        int zlo = 0, zhi = 0;
+        if (g.od < d) {
+            zlo = zhi = gi[g.od];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                zlo = min(zlo, __shfl_xor_sync(0xffffffffu, zlo, o));
+                zhi = max(zhi, __shfl_xor_sync(0xffffffffu, zhi, o));
+            }
+        }
+        for (int s0 = 0; s0 < nst; s0 += 32) {
+            const int s = s0 + lane;
+            int cb = 0, ce = 0;
+            if (s < nst) {
+                bool inb = true;
+                for (int l = 0; l < g.od; l++) {
+                    const int v = gi[l] + __ldg(w.st_off + (size_t)s * g.od + l);
+                    inb = inb && (unsigned)v < (unsigned)g.width;
+                }
+                if (inb) {
+                    const int o = obase + __ldg(w.st_delta + s);
+                    cb = __ldg(w.outer_begin + o);
+                    ce = __ldg(w.outer_begin + o + 1);
+                    if (cb < ce && g.od < d) {
+                        const int* keys = w.cell_dims + (size_t)g.od * g.ns;
+                        cb = lower_bound_i(keys, cb, ce, zlo - g.r - 1);
+                        ce = lower_bound_i(keys, cb, ce, zhi + g.r + 2);
+                    }
+                }
+            }
+            unsigned live = __ballot_sync(0xffffffffu, cb < ce);
+            while (live) {
+                const int src = __ffs(live) - 1;
+                live &= live - 1;
+                const int b = __shfl_sync(0xffffffffu, cb, src);
+                const int e = __shfl_sync(0xffffffffu, ce, src);
+                for (int c = b; c < e; c++) fn(c);
+            }
+        }
+    } else {
+        for (int s = 0; s < nst; s++) {
+            bool inb = true;
+            for (int l = 0; l < g.od; l++) {
+                const int v = gi[l] + __ldg(w.st_off + (size_t)s * g.od + l);
+                inb = inb && (unsigned)v < (unsigned)g.width;
+            }
+            if (!inb) continue;
+            const int o = obase + __ldg(w.st_delta + s);
+            int cb = __ldg(w.outer_begin + o), ce = __ldg(w.outer_begin + o + 1);
+            if (cb >= ce) continue;
+            if (g.od < d) {
+                const int* keys = w.cell_dims + (size_t)g.od * g.ns;
+                cb = lower_bound_i(keys, cb, ce, gi[g.od] - g.r - 1);
+                ce = lower_bound_i(keys, cb, ce, gi[g.od] + g.r + 2);
+            }
+            for (int c = cb; c < ce; c++) fn(c);
+        }
+    }
+}
+
+}  // namespace egg

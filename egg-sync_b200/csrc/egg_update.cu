@@ -21,6 +21,7 @@
 // the reference exactly (EGG_SynC.cu:583-597, 613-636, 666-681, 706-709).
 #include "egg_common.cuh"
 #include "egg_kernels.h"
+#include "egg_stencil.cuh"
 
 namespace egg {
 
@@ -262,68 +263,8 @@ __global__ void __launch_bounds__(128) k_update(Geom g, Work w, int* __restrict_
     const int own = w.cell_of[iv];
     const int own_cnt = w.cell_start[own + 1] - w.cell_start[own];
 
-    const int nst = w.st_count[0];
-    const int ob0 = __shfl_sync(0xffffffffu, obase, 0);
-    if (__all_sync(0xffffffffu, obase == ob0)) {
-        int zlo = 0, zhi = 0;
-        if (g.od < d) {
-            zlo = zhi = gi[g.od];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                zlo = min(zlo, __shfl_xor_sync(0xffffffffu, zlo, o));
-                zhi = max(zhi, __shfl_xor_sync(0xffffffffu, zhi, o));
-            }
-        }
-        for (int s0 = 0; s0 < nst; s0 += 32) {
-            const int s = s0 + lane;
-            int cb = 0, ce = 0;
-            if (s < nst) {
-                bool inb = true;
-                for (int l = 0; l < g.od; l++) {
-                    const int v = gi[l] + __ldg(w.st_off + (size_t)s * g.od + l);
-                    inb = inb && (unsigned)v < (unsigned)g.width;
-                }
-                if (inb) {
-                    const int o = obase + __ldg(w.st_delta + s);
-                    cb = __ldg(w.outer_begin + o);
-                    ce = __ldg(w.outer_begin + o + 1);
-                    if (cb < ce && g.od < d) {
-                        // cells beyond r+1 in dimension od fail the box test
-                        // (their gap exceeds (r+1)*side > eps) for every lane
-                        const int* keys = w.cell_dims + (size_t)g.od * g.ns;
-                        cb = lower_bound_i(keys, cb, ce, zlo - g.r - 1);
-                        ce = lower_bound_i(keys, cb, ce, zhi + g.r + 2);
-                    }
-                }
-            }
-            unsigned live = __ballot_sync(0xffffffffu, cb < ce);
-            while (live) {
-                const int src = __ffs(live) - 1;
-                live &= live - 1;
-                const int b = __shfl_sync(0xffffffffu, cb, src);
-                const int e = __shfl_sync(0xffffffffu, ce, src);
-                for (int c = b; c < e; c++) visit_cell<D>(g, w, c, x, gi, a, Ts, Tc, Tm, K, TW);
-            }
-        }
-    } else {
-        for (int s = 0; s < nst; s++) {
-            bool inb = true;
-            for (int l = 0; l < g.od; l++) {
-                const int v = gi[l] + __ldg(w.st_off + (size_t)s * g.od + l);
-                inb = inb && (unsigned)v < (unsigned)g.width;
-            }
-            if (!inb) continue;
-            const int o = obase + __ldg(w.st_delta + s);
-            int cb = __ldg(w.outer_begin + o), ce = __ldg(w.outer_begin + o + 1);
-            if (cb >= ce) continue;
-            if (g.od < d) {
-                const int* keys = w.cell_dims + (size_t)g.od * g.ns;
-                cb = lower_bound_i(keys, cb, ce, gi[g.od] - g.r - 1);
-                ce = lower_bound_i(keys, cb, ce, gi[g.od] + g.r + 2);
-            }
-            for (int c = cb; c < ce; c++) visit_cell<D>(g, w, c, x, gi, a, Ts, Tc, Tm, K, TW);
-        }
-    }
+    for_candidates(g, w, gi, obase, lane, d,
+                   [&](int c) { visit_cell<D>(g, w, c, x, gi, a, Ts, Tc, Tm, K, TW); });
 
     const int N = a.N;
     const float fN = (float)N;

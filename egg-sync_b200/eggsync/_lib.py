@@ -29,7 +29,7 @@ EXPORTS = ("egg_opts_default", "egg_sync_run", "egg_sync_step", "egg_sync_grid",
 class EggOpts(C.Structure):
     _fields_ = [("max_iter", C.c_int32), ("loop", C.c_int32), ("stop_rule", C.c_int32),
                 ("order_param", C.c_int32), ("profile", C.c_int32), ("full_update", C.c_int32),
-                ("positions_out", C.c_void_p), ("reserved", C.c_int32 * 8)]
+                ("positions_out", C.c_void_p), ("labels_mode", C.c_int32), ("reserved", C.c_int32 * 7)]
 
 
 class EggStats(C.Structure):
@@ -37,7 +37,9 @@ class EggStats(C.Structure):
                 ("n_clusters", C.c_int32), ("extra_checks", C.c_int32), ("status_bits", C.c_int32),
                 ("workspace_bytes", C.c_int64), ("order_param", C.c_double), ("stage_ms", C.c_float * 6),
                 ("total_ms", C.c_float), ("itr_ms", C.POINTER(C.c_float)), ("itr_cap", C.c_int32),
-                ("kernel_ms", C.c_float * 4), ("kernel_launches", C.c_int32 * 4), ("launches", C.c_int32)]
+                ("kernel_ms", C.c_float * 4), ("kernel_launches", C.c_int32 * 4), ("launches", C.c_int32),
+                ("order_param_lo", C.c_double), ("order_param_hi", C.c_double),
+                ("itr_order_param", C.POINTER(C.c_double))]
 
 
 class EggError(RuntimeError):

@@ -91,7 +91,8 @@ def _out_ptr(buf, n, dtype_np, what):
 
 def egg_sync(D, eps: float, lam: float = DEFAULT_LAMBDA, max_iter: int = 0, loop: str = "graph",
              labels_out=None, profile: bool = False, full_update: bool = False,
-             positions_out=None) -> Tuple[object, dict]:
+             positions_out=None, stop_rule: str = "flag", order_param: int = 0,
+             labels_mode: str = "union_find") -> Tuple[object, dict]:
     """Run EGG-SynC; return (int32 labels, stats dict).
 
     ``labels_out`` may be a preallocated int32 numpy array or torch tensor
@@ -101,7 +102,10 @@ def egg_sync(D, eps: float, lam: float = DEFAULT_LAMBDA, max_iter: int = 0, loop
     recomputes every point in every iteration (the default reuses results
     whose inputs did not change; both give identical bits).
     ``positions_out`` (optional n x d float32 buffer) receives the final
-    positions."""
+    positions.  ``stop_rule`` "flag" is the reference EGG-SynC's convergence
+    test; "lambda" stops once the certified lower bound of the FP64 local
+    order parameter reaches ``lam``.  ``order_param`` 1 reports the order
+    parameter of the final positions, 2 that of every iteration."""
     L = _lib.load()
     ptr, n, d, keep, dev, stream = _prepare(D)
     if labels_out is None:
@@ -113,6 +117,9 @@ def egg_sync(D, eps: float, lam: float = DEFAULT_LAMBDA, max_iter: int = 0, loop
     opts.loop = {"graph": 0, "host": 1}[loop]
     opts.profile = 1 if profile else 0
     opts.full_update = 1 if full_update else 0
+    opts.stop_rule = {"flag": 0, "lambda": 1}[stop_rule]
+    opts.order_param = int(order_param)
+    opts.labels_mode = {"union_find": 0, "cells": 1}[labels_mode]
     if positions_out is not None:
         opts.positions_out = _out_ptr(positions_out, n * d, np.float32, "positions_out")
     stats = EggStats()
@@ -120,6 +127,8 @@ def egg_sync(D, eps: float, lam: float = DEFAULT_LAMBDA, max_iter: int = 0, loop
     itr = (C.c_float * cap)()
     stats.itr_ms = C.cast(itr, C.POINTER(C.c_float))
     stats.itr_cap = cap
+    itr_r = (C.c_double * (2 * cap))()
+    stats.itr_order_param = C.cast(itr_r, C.POINTER(C.c_double))
     with _DeviceGuard(dev):
         st = check(L.egg_sync_run(C.c_void_p(ptr), n, d, float(eps), float(lam), C.byref(opts), C.c_void_p(lptr),
                                   C.byref(stats), C.c_void_p(stream) if stream else None))
@@ -140,6 +149,10 @@ def egg_sync(D, eps: float, lam: float = DEFAULT_LAMBDA, max_iter: int = 0, loop
         "kernel_launches": dict(zip(("build", "cell_sums", "update", "extra"),
                                     [int(v) for v in stats.kernel_launches])),
         "launches": int(stats.launches),
+        "order_param": (float(stats.order_param_lo), float(stats.order_param_hi)),
+        "itr_order_param": [(float(itr_r[2 * k]), float(itr_r[2 * k + 1]))
+                            for k in range(min(stats.iterations, cap))] if (order_param == 2 or
+                                                                             stop_rule == "lambda") else [],
     }
     return labels_out, info
 

@@ -38,13 +38,17 @@ typedef struct egg_opts {
                              1 = host-driven loop (one 4-byte readback per iteration) */
     int32_t stop_rule;    /* 0 = the reference's convergence flag (EGG_SynC.cu:1322),
                              1 = local order parameter >= lam (SynC.cpp:277-303 semantics) */
-    int32_t order_param;  /* 0 = off, 1 = report the final FP64 order parameter */
+    int32_t order_param;  /* FP64 local order parameter r = mean_p mean_{q in N(p)} exp(-|p-q|)
+                             (SynC.cpp:42-56) over the update's neighbourhoods, as certified bounds:
+                             0 = off, 1 = of the final positions, 2 = every iteration */
     int32_t profile;      /* 1 = time every kernel group with CUDA events (host-driven loop) */
     int32_t full_update;  /* 1 = recompute every point in every iteration.  By default a point whose
                              whole stencil region held no moved point since the last update keeps
                              its previous result, which is bit-identical to recomputing it. */
     float *positions_out; /* optional n x d buffer (host or device): final positions, input order */
-    int32_t reserved[8];
+    int32_t labels_mode;  /* 0 = GPU union-find over the points of each final cell (default),
+                             1 = direct per-cell labelling; both give identical labels */
+    int32_t reserved[7];
 } egg_opts;
 
 typedef struct egg_stats {
@@ -65,6 +69,11 @@ typedef struct egg_stats {
                               sums, update and extra-check kernel groups */
     int32_t kernel_launches[4];  /* launches of each group's main kernel */
     int32_t launches;      /* kernels the call launched (all groups, loop control included) */
+    double order_param_lo; /* certified FP64 bounds of the local order parameter (final value with
+                              opts->order_param == 1, last iteration's with 2 or stop_rule 1), else -1 */
+    double order_param_hi;
+    double *itr_order_param; /* optional caller array of 2*itr_cap doubles: [lo, hi] per iteration
+                                (opts->order_param == 2 or stop_rule == 1) */
 } egg_stats;
 
 /* Fill *opts with the defaults (all zero). */

@@ -343,7 +343,17 @@ typedef struct {
     int count;        /* |N_eps(p)| */
     int half;         /* reference half_count */
     int partial_in;   /* neighbours found in partial cells */
+    double rsum;      /* sum over N_eps(p) of exp(-|x_p - x_q|) (FP64) */
 } step_ctx;
+
+static inline double exp_neg_dist(const float *a, const float *b, int d) {
+    double s = 0.0;
+    for (int l = 0; l < d; l++) {
+        double df = (double)a[l] - (double)b[l];
+        s += df * df;
+    }
+    return exp(-sqrt(s));
+}
 
 static void step_visit(const grid_t *G, int c, void *vctx) {
     step_ctx *s = (step_ctx *)vctx;
@@ -356,6 +366,7 @@ static void step_visit(const grid_t *G, int c, void *vctx) {
         for (int i = b; i < e; i++) {
             const float *xq = &G->X[(size_t)G->order[i] * d];
             for (int l = 0; l < d; l++) s->sum[l] += sin((double)xq[l] - (double)s->xp[l]);
+            s->rsum += exp_neg_dist(s->xp, xq, d);
         }
         s->count += e - b;
         if (s->border) {
@@ -369,6 +380,7 @@ static void step_visit(const grid_t *G, int c, void *vctx) {
             const float *xq = &G->X[(size_t)G->order[i] * d];
             if (pdist2(s->xp, xq, d) <= G->g.t_eps) {
                 for (int l = 0; l < d; l++) s->sum[l] += sin((double)xq[l] - (double)s->xp[l]);
+                s->rsum += exp_neg_dist(s->xp, xq, d);
                 s->count++;
                 s->partial_in++;
             }
@@ -429,6 +441,26 @@ ORACLE_API int egg_oracle_step_sample(const float *X, int n, int d, float eps, c
     }
     grid_free(&G);
     return 0;
+}
+
+/* Local order parameter over the EGG-SynC neighbourhoods (the update's cells
+ * and tests), exact in FP64: mean_p mean_{q in N(p)} exp(-|x_p - x_q|), the
+ * quantity of SynC.cpp:42-56 on the neighbourhoods the loop actually uses. */
+ORACLE_API double egg_oracle_order_parameter_egg(const float *X, int n, int d, float eps) {
+    grid_t G;
+    if (d > 64 || grid_build(&G, X, n, d, eps) != 0) return -1.0;
+    double total = 0.0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : total)
+    for (int p = 0; p < n; p++) {
+        step_ctx s;
+        memset(&s, 0, sizeof(s));
+        s.xp = &X[(size_t)p * d];
+        s.p_cell = G.cell_of_pt[p];
+        visit_stencil(&G, &G.gid[(size_t)p * d], G.g.r, step_visit, &s);
+        total += s.rsum / (double)s.count;
+    }
+    grid_free(&G);
+    return total / n;
 }
 
 /* ------------------------------ extra check ------------------------------ */

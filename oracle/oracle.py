@@ -68,6 +68,8 @@ class Oracle:
         L.egg_oracle_update_sample.argtypes = [_f32p, C.c_int, C.c_int, C.c_float, _i32p, C.c_int, _f32p, _i32p]
         L.egg_oracle_order_parameter.argtypes = [_f32p, C.c_int, C.c_int, C.c_float]
         L.egg_oracle_order_parameter.restype = C.c_double
+        L.egg_oracle_order_parameter_egg.argtypes = [_f32p, C.c_int, C.c_int, C.c_float]
+        L.egg_oracle_order_parameter_egg.restype = C.c_double
         L.egg_oracle_threads.restype = C.c_int
         L.egg_oracle_step_sample.argtypes = [_f32p, C.c_int, C.c_int, C.c_float, _i32p, C.c_int, _f32p, _i32p,
                                              _i32p]
@@ -165,8 +167,14 @@ class Oracle:
         return out, cnt
 
     def order_parameter(self, X, eps):
+        """Brute-force neighbourhoods (the reference CPU SynC's)."""
         X = _as_x(X)
         return self.L.egg_oracle_order_parameter(X, X.shape[0], X.shape[1], float(eps))
+
+    def order_parameter_egg(self, X, eps):
+        """Neighbourhoods of the EGG-SynC update (exact FP64)."""
+        X = _as_x(X)
+        return self.L.egg_oracle_order_parameter_egg(X, X.shape[0], X.shape[1], float(eps))
 
 
 class RefSync:

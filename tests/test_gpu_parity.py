@@ -114,6 +114,52 @@ def test_incremental_equals_full_update(name):
     assert np.array_equal(pa.view(np.uint32), pb.view(np.uint32))
 
 
+@pytest.mark.parametrize("name", ["c1_s0", "c3a_s0", "duplicates", "noise", "d1"])
+def test_union_find_labels_equal_cell_labels(name):
+    """GPU union-find cluster extraction gives the reference's partition and
+    label values (the direct per-cell labelling)."""
+    X, eps = CASES[name]
+    a, ia = egg_sync(X, eps)  # union-find (default)
+    b, ib = egg_sync(X, eps, labels_mode="cells")
+    assert np.array_equal(a, b)
+    assert ia["n_clusters"] == ib["n_clusters"] == len(np.unique(a[a >= 0]))
+
+
+@pytest.mark.parametrize("name", ["c1_s0", "c3a_s0", "noise", "d5"])
+def test_order_parameter_bounds_contain_exact(oracle, name):
+    """The certified FP64 interval of the local order parameter contains the
+    exact value over the same neighbourhoods (oracle), on the input and on
+    the final positions."""
+    X, eps = CASES[name]
+    # of the input: one iteration with the every-iteration mode
+    _, info = egg_sync(X, eps, max_iter=1, order_param=2)
+    lo, hi = info["itr_order_param"][0]
+    exact = oracle.order_parameter_egg(X, eps)
+    assert lo <= exact <= hi and hi - lo < 0.05
+    # of the final positions
+    P = np.empty_like(X)
+    lab, info = egg_sync(X, eps, order_param=1, positions_out=P)
+    lo, hi = info["order_param"]
+    exact = oracle.order_parameter_egg(P, eps)
+    assert lo <= exact <= hi
+    assert hi - lo < 1e-4  # collapsed clusters: the interval is tight
+    # reporting does not change the run
+    lab2, info2 = egg_sync(X, eps)
+    assert np.array_equal(lab, lab2) and info2["iterations"] == info["iterations"]
+
+
+def test_lambda_stop_rule():
+    """stop_rule="lambda" stops at the first iteration whose certified lower
+    bound reaches lambda (SynC.cpp:277-303 semantics on the EGG neighbourhoods)."""
+    X, eps = CASES["c1_s0"]
+    lab, info = egg_sync(X, eps, lam=0.999, stop_rule="lambda")
+    r = info["itr_order_param"]
+    assert info["converged"] and len(r) == info["iterations"]
+    assert r[-1][0] >= 0.999
+    assert all(lo < 0.999 for lo, _ in r[:-1])
+    assert all(lo <= hi for lo, hi in r)
+
+
 def test_deterministic_and_loop_modes():
     X, eps = CASES["c1_s0"]
     a, ia = egg_sync(X, eps)
