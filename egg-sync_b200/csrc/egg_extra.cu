@@ -97,15 +97,15 @@ __device__ bool mbr_exact(const Geom& g, const Work& w, int qi, const float* xp)
 
 // extremes of each point's eps/2 group (itself included)
 template <int D>
-__global__ void __launch_bounds__(128) k_ball_bbox(Geom g, Work w) {
+__device__ __forceinline__ void ball_bbox_body(const Geom& g, const Work& w, int bx, int gx) {
     constexpr int DM = D > 0 ? D : kMaxDims;
     const int d = D > 0 ? D : g.d;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (bx == 0 && threadIdx.x == 0) {
         const int it = w.ctrl[kCtrlIter];
         w.stamps[4 * it + 2] = globaltimer();
     }
     if (w.ctrl[kCtrlFlag] == 0) return;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+    for (int i = bx * blockDim.x + threadIdx.x; i < g.n; i += gx * blockDim.x) {
         float xq[DM], lo[DM], hi[DM];
         int gq[DM];
         int obase = 0;
@@ -154,10 +154,10 @@ __global__ void __launch_bounds__(128) k_ball_bbox(Geom g, Work w) {
 // Union over a cell's points of their eps/2-group extremes.  The MBR of any
 // pair (p, q) with q in the cell lies inside it, so its distance to p is a
 // lower bound for every pair of the cell.
-__global__ void __launch_bounds__(256) k_cell_ballbox(Geom g, Work w) {
+__device__ __forceinline__ void cell_ballbox_body(const Geom& g, const Work& w, int bx, int gx) {
     if (w.ctrl[kCtrlFlag] == 0) return;
     const int M = w.ctrl[kCtrlM];
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < M; c += gridDim.x * blockDim.x) {
+    for (int c = bx * blockDim.x + threadIdx.x; c < M; c += gx * blockDim.x) {
         const int qb = w.cell_start[c], qe = w.cell_start[c + 1];
         for (int l = 0; l < g.d; l++) {
             float lo = 3.0e38f, hi = -3.0e38f;
@@ -172,13 +172,13 @@ __global__ void __launch_bounds__(256) k_cell_ballbox(Geom g, Work w) {
 }
 
 template <int D>
-__global__ void __launch_bounds__(128) k_annulus(Geom g, Work w) {
+__device__ __forceinline__ void annulus_body(const Geom& g, const Work& w, int bx, int gx) {
     constexpr int DM = D > 0 ? D : kMaxDims;
     const int d = D > 0 ? D : g.d;
     volatile int* flag = w.ctrl + kCtrlFlag;
     if (*flag == 0) return;
     int pairs = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+    for (int i = bx * blockDim.x + threadIdx.x; i < g.n; i += gx * blockDim.x) {
         float xp[DM];
         int gp[DM];
         int obase = 0;
@@ -232,6 +232,26 @@ __global__ void __launch_bounds__(128) k_annulus(Geom g, Work w) {
     if (pairs) atomicAdd(w.ctrl + kCtrlPairs, pairs);
 }
 
+template <int D>
+__global__ void __launch_bounds__(128) k_ball_bbox(Geom g, Work w) { ball_bbox_body<D>(g, w, blockIdx.x, gridDim.x); }
+template <int D>
+__global__ void __launch_bounds__(128) kb_ball_bbox(BatchArgs B, int skip) {
+    EGG_BATCH_ENTRY(B, skip);
+    ball_bbox_body<D>(g, w, bx, gx);
+}
+__global__ void __launch_bounds__(256) k_cell_ballbox(Geom g, Work w) { cell_ballbox_body(g, w, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(256) kb_cell_ballbox(BatchArgs B, int skip) {
+    EGG_BATCH_ENTRY(B, skip);
+    cell_ballbox_body(g, w, bx, gx);
+}
+template <int D>
+__global__ void __launch_bounds__(128) k_annulus(Geom g, Work w) { annulus_body<D>(g, w, blockIdx.x, gridDim.x); }
+template <int D>
+__global__ void __launch_bounds__(128) kb_annulus(BatchArgs B, int skip) {
+    EGG_BATCH_ENTRY(B, skip);
+    annulus_body<D>(g, w, bx, gx);
+}
+
 #define EGG_DISPATCH_D(d, KERNEL, ...)                \
     switch (d) {                                      \
         case 1: KERNEL<1> __VA_ARGS__; break;         \
@@ -247,13 +267,18 @@ __global__ void __launch_bounds__(128) k_annulus(Geom g, Work w) {
 
 // Both kernels return at once unless the update left the flag at 1; the
 // grids are bounded so that the common early exit costs little.
-void launch_extra_check(const Geom& g, const Work& w, cudaStream_t st) {
-    const int threads = 128;
-    int blocks = (g.n + threads - 1) / threads;
-    if (blocks > 148 * 8) blocks = 148 * 8;
-    EGG_DISPATCH_D(g.d, k_ball_bbox, <<<blocks, threads, 0, st>>>(g, w));
-    k_cell_ballbox<<<blocks, 256, 0, st>>>(g, w);
-    EGG_DISPATCH_D(g.d, k_annulus, <<<blocks, threads, 0, st>>>(g, w));
+void launch_extra_check(const Exec& ex, cudaStream_t st) {
+    const int blocks = ex.blocks(kShapeCapN128);
+    if (ex.batch()) {
+        const BatchArgs B = ex.args(kShapeCapN128);
+        EGG_DISPATCH_D(ex.d, kb_ball_bbox, <<<blocks, 128, 0, st>>>(B, ex.skip_done));
+        kb_cell_ballbox<<<blocks, 256, 0, st>>>(B, ex.skip_done);
+        EGG_DISPATCH_D(ex.d, kb_annulus, <<<blocks, 128, 0, st>>>(B, ex.skip_done));
+    } else {
+        EGG_DISPATCH_D(ex.d, k_ball_bbox, <<<blocks, 128, 0, st>>>(*ex.g, *ex.w));
+        k_cell_ballbox<<<blocks, 256, 0, st>>>(*ex.g, *ex.w);
+        EGG_DISPATCH_D(ex.d, k_annulus, <<<blocks, 128, 0, st>>>(*ex.g, *ex.w));
+    }
 }
 
 }  // namespace egg

@@ -16,6 +16,9 @@
 // cell digit from the positions through the current permutation.  All
 // passes are stable and run in a fixed order, so the whole index (and the
 // cell sums below) is bit-reproducible from run to run.
+//
+// Every kernel is a device body over its block index (bx, gx) with a
+// single-instance wrapper and a batched wrapper (egg_batch.cuh).
 #include "egg_common.cuh"
 #include "egg_kernels.h"
 
@@ -86,7 +89,28 @@ __device__ __forceinline__ int digit_of(const Geom& g, const float* __restrict__
     return dig;
 }
 
+// permutation buffer of a sort pass: 0 = perm, 1 = perm_tmp
+__device__ __forceinline__ int* perm_buf(const Work& w, int sel) { return sel ? w.perm_tmp : w.perm; }
+
+struct TwoSum {
+    float hi, lo;
+};
+
+__device__ __forceinline__ TwoSum ts_add(TwoSum a, TwoSum b) {
+    float s = __fadd_rn(a.hi, b.hi);
+    float bb = __fsub_rn(s, a.hi);
+    float err = __fadd_rn(__fsub_rn(a.hi, __fsub_rn(s, bb)), __fsub_rn(b.hi, bb));
+    return {s, __fadd_rn(__fadd_rn(a.lo, b.lo), err)};
+}
+
+__device__ __forceinline__ size_t wp_idx(int field, int l, int d, int rec, int nw, int warp) {
+    return wp_idx_f(field, l, d, rec, nw, warp);
+}
+
 }  // namespace
+
+#define EGG_SKIP_IF_UNCHANGED(ctrl) \
+    if ((ctrl)[kCtrlChanged] == 0) return;
 
 // ---------------------------------------------------------------------------
 // has any point left its cell?  A stable sort of unchanged keys is the
@@ -95,11 +119,11 @@ __device__ __forceinline__ int digit_of(const Geom& g, const float* __restrict__
 // kernel below returns at once.  Also copies the positions into X.
 // ---------------------------------------------------------------------------
 template <int D>
-__global__ void __launch_bounds__(256) k_check_cells(Geom g, Work w) {
+__device__ __forceinline__ void check_cells_body(const Geom& g, const Work& w, int bx, int gx) {
     const int d = D > 0 ? D : g.d;
     const bool valid = w.ctrl[kCtrlGridValid] != 0;
     bool changed = false;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+    for (int i = bx * blockDim.x + threadIdx.x; i < g.n; i += gx * blockDim.x) {
         const int c = valid ? w.cell_of[i] : 0;
         for (int l = 0; l < d; l++) {
             const float x = w.Xn[(size_t)l * g.ns + i];
@@ -109,48 +133,42 @@ __global__ void __launch_bounds__(256) k_check_cells(Geom g, Work w) {
     }
     if (!valid) changed = true;
     // the incremental update's need marks are rebuilt after every grid check
-    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < g.n_outer; o += gridDim.x * blockDim.x) w.need[o] = 0;
+    for (int o = bx * blockDim.x + threadIdx.x; o < g.n_outer; o += gx * blockDim.x) w.need[o] = 0;
     if (__syncthreads_or(changed) && threadIdx.x == 0) w.ctrl[kCtrlChanged] = 1;
 }
 
-__global__ void k_build_begin(int* ctrl) {
-    ctrl[kCtrlChanged] = 0;
-    ctrl[kCtrlSpanCount] = 0;
-    ctrl[kCtrlBigCount] = 0;
+__device__ __forceinline__ void build_begin_body(const Work& w) {
+    w.ctrl[kCtrlChanged] = 0;
+    w.ctrl[kCtrlSpanCount] = 0;
+    w.ctrl[kCtrlBigCount] = 0;
 }
 
-#define EGG_SKIP_IF_UNCHANGED(ctrl) \
-    if ((ctrl)[kCtrlChanged] == 0) return;
-
-// ---------------------------------------------------------------------------
 // radix sort pass: tile histograms
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kSortThreads) k_radix_hist(Geom g, const float* __restrict__ Xs,
-                                                             const int* __restrict__ pin, int first, int dim,
-                                                             int shift, int* __restrict__ hist, int tiles,
-                                                             const int* __restrict__ ctrl) {
-    EGG_SKIP_IF_UNCHANGED(ctrl);
+__device__ __forceinline__ void radix_hist_body(const Geom& g, const Work& w, int in_sel, int first, int dim, int shift, int bx) {
+    EGG_SKIP_IF_UNCHANGED(w.ctrl);
     __shared__ int h[256];
+    const int tiles = (g.n + kSortTile - 1) / kSortTile;
+    const int* pin = perm_buf(w, in_sel);
     for (int t = threadIdx.x; t < 256; t += blockDim.x) h[t] = 0;
     __syncthreads();
-    const int base = blockIdx.x * kSortTile;
+    const int base = bx * kSortTile;
     const int end = min(base + kSortTile, g.n);
     for (int i = base + threadIdx.x; i < end; i += blockDim.x) {
         int j = first ? i : __ldg(pin + i);
-        int dg = digit_of(g, Xs, j, dim, shift);
+        int dg = digit_of(g, w.Xn, j, dim, shift);
         unsigned act = __activemask();
         unsigned peers = __match_any_sync(act, dg);
         if ((peers & lanemask_lt()) == 0) atomicAdd(&h[dg], __popc(peers));
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < 256; t += blockDim.x) hist[(size_t)t * tiles + blockIdx.x] = h[t];
+    for (int t = threadIdx.x; t < 256; t += blockDim.x) w.hist[(size_t)t * tiles + bx] = h[t];
 }
 
 // per-digit exclusive scan over tiles (one block per digit)
-__global__ void __launch_bounds__(256) k_radix_scan(int* __restrict__ hist, int tiles, int* __restrict__ digit_total,
-                                                    const int* __restrict__ ctrl) {
-    EGG_SKIP_IF_UNCHANGED(ctrl);
-    int* h = hist + (size_t)blockIdx.x * tiles;
+__device__ __forceinline__ void radix_scan_body(const Geom& g, const Work& w, int bx) {
+    EGG_SKIP_IF_UNCHANGED(w.ctrl);
+    const int tiles = (g.n + kSortTile - 1) / kSortTile;
+    int* h = w.hist + (size_t)bx * tiles;
     const int per = (tiles + blockDim.x - 1) / blockDim.x;
     const int b = threadIdx.x * per;
     const int e = min(b + per, tiles);
@@ -163,31 +181,31 @@ __global__ void __launch_bounds__(256) k_radix_scan(int* __restrict__ hist, int 
         h[k] = run;
         run += v;
     }
-    if (threadIdx.x == 0) digit_total[blockIdx.x] = total;
+    if (threadIdx.x == 0) w.digit_total[bx] = total;
 }
 
 // stable scatter of one tile
-__global__ void __launch_bounds__(kSortThreads) k_radix_scatter(Geom g, const float* __restrict__ Xs,
-                                                                const int* __restrict__ pin, int first, int dim,
-                                                                int shift, const int* __restrict__ hist,
-                                                                const int* __restrict__ digit_total, int tiles,
-                                                                int* __restrict__ pout, const int* __restrict__ ctrl) {
-    EGG_SKIP_IF_UNCHANGED(ctrl);
+__device__ __forceinline__ void radix_scatter_body(const Geom& g, const Work& w, int in_sel, int out_sel, int first, int dim, int shift,
+                                   int bx) {
+    EGG_SKIP_IF_UNCHANGED(w.ctrl);
     constexpr int kWarps = kSortThreads / 32;
     __shared__ int base[256];
     __shared__ int run[256];
     __shared__ int wcnt[kWarps][256];
+    const int tiles = (g.n + kSortTile - 1) / kSortTile;
+    const int* pin = perm_buf(w, in_sel);
+    int* pout = perm_buf(w, out_sel);
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     {
-        int v = digit_total[tid];
+        int v = w.digit_total[tid];
         int db = block_exclusive_scan(v, nullptr);
-        base[tid] = db + hist[(size_t)tid * tiles + blockIdx.x];
+        base[tid] = db + w.hist[(size_t)tid * tiles + bx];
         run[tid] = 0;
 #pragma unroll
-        for (int w = 0; w < kWarps; w++) wcnt[w][tid] = 0;
+        for (int k = 0; k < kWarps; k++) wcnt[k][tid] = 0;
     }
     __syncthreads();
-    const int tile0 = blockIdx.x * kSortTile;
+    const int tile0 = bx * kSortTile;
     for (int round = 0; round < kSortTile / kSortThreads; round++) {
         const int i = tile0 + round * kSortThreads + tid;
         if (tile0 + round * kSortThreads >= g.n) break;  // uniform across the block
@@ -195,7 +213,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(Geom g, const fl
         int j = 0, dg = 0;
         if (valid) {
             j = first ? i : __ldg(pin + i);
-            dg = digit_of(g, Xs, j, dim, shift);
+            dg = digit_of(g, w.Xn, j, dim, shift);
         }
         unsigned peers = __match_any_sync(0xffffffffu, valid ? dg : 256 + lane);
         int rank = __popc(peers & lanemask_lt());
@@ -204,9 +222,9 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(Geom g, const fl
         {
             int r = run[tid];
 #pragma unroll
-            for (int w = 0; w < kWarps; w++) {
-                int c = wcnt[w][tid];
-                wcnt[w][tid] = r;
+            for (int k = 0; k < kWarps; k++) {
+                int c = wcnt[k][tid];
+                wcnt[k][tid] = r;
                 r += c;
             }
             run[tid] = r;
@@ -215,19 +233,17 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(Geom g, const fl
         if (valid) pout[base[dg] + wcnt[wid][dg] + rank] = j;
         __syncthreads();
 #pragma unroll
-        for (int w = 0; w < kWarps; w++) wcnt[w][tid] = 0;
+        for (int k = 0; k < kWarps; k++) wcnt[k][tid] = 0;
         __syncthreads();
     }
 }
 
-// ---------------------------------------------------------------------------
 // gather into the new order and count cell heads per block
-// ---------------------------------------------------------------------------
 template <int D>
-__global__ void __launch_bounds__(kHeadsBlock) k_gather_heads(Geom g, Work w, int identity) {
+__device__ __forceinline__ void gather_heads_body(const Geom& g, const Work& w, int identity, int bx) {
     EGG_SKIP_IF_UNCHANGED(w.ctrl);
     const int d = D > 0 ? D : g.d;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = bx * blockDim.x + threadIdx.x;
     int head = 0;
     if (i < g.n) {
         const int j = identity ? i : __ldg(w.perm + i);
@@ -245,12 +261,14 @@ __global__ void __launch_bounds__(kHeadsBlock) k_gather_heads(Geom g, Work w, in
     }
     int total;
     block_exclusive_scan(head, &total);
-    if (threadIdx.x == 0) w.block_sums[blockIdx.x] = total;
+    if (threadIdx.x == 0) w.block_sums[bx] = total;
 }
 
 // single-block exclusive scan of the per-block head counts; M = total
-__global__ void __launch_bounds__(1024) k_scan_block_sums(int* __restrict__ bs, int nb, int* __restrict__ ctrl) {
-    EGG_SKIP_IF_UNCHANGED(ctrl);
+__device__ __forceinline__ void scan_block_sums_body(const Geom& g, const Work& w) {
+    EGG_SKIP_IF_UNCHANGED(w.ctrl);
+    const int nb = (g.n + kHeadsBlock - 1) / kHeadsBlock;
+    int* bs = w.block_sums;
     const int per = (nb + blockDim.x - 1) / blockDim.x;
     const int b = threadIdx.x * per;
     const int e = min(b + per, nb);
@@ -264,17 +282,17 @@ __global__ void __launch_bounds__(1024) k_scan_block_sums(int* __restrict__ bs, 
         run += v;
     }
     if (threadIdx.x == 0) {
-        ctrl[kCtrlM] = total;
-        ctrl[kCtrlGridValid] = 1;
-        ctrl[kCtrlBuilds] += 1;
+        w.ctrl[kCtrlM] = total;
+        w.ctrl[kCtrlGridValid] = 1;
+        w.ctrl[kCtrlBuilds] += 1;
     }
 }
 
 template <int D>
-__global__ void __launch_bounds__(kHeadsBlock) k_heads_finalize(Geom g, Work w) {
+__device__ __forceinline__ void heads_finalize_body(const Geom& g, const Work& w, int bx) {
     EGG_SKIP_IF_UNCHANGED(w.ctrl);
     const int d = D > 0 ? D : g.d;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = bx * blockDim.x + threadIdx.x;
     int head = 0;
     if (i < g.n) {
         head = (i == 0);
@@ -282,7 +300,7 @@ __global__ void __launch_bounds__(kHeadsBlock) k_heads_finalize(Geom g, Work w) 
             for (int l = 0; l < d && !head; l++)
                 head = cell_dim(w.X[(size_t)l * g.ns + i], g) != cell_dim(w.X[(size_t)l * g.ns + i - 1], g);
     }
-    int excl = block_exclusive_scan(head, nullptr) + w.block_sums[blockIdx.x];
+    int excl = block_exclusive_scan(head, nullptr) + w.block_sums[bx];
     if (i < g.n) {
         const int c = excl + head - 1;
         w.cell_of[i] = c;
@@ -302,10 +320,10 @@ __global__ void __launch_bounds__(kHeadsBlock) k_heads_finalize(Geom g, Work w) 
 }
 
 // outer_begin[o] = first cell whose outer id >= o, o in [0, n_outer]
-__global__ void k_outer_ranges(Geom g, Work w) {
+__device__ __forceinline__ void outer_ranges_body(const Geom& g, const Work& w, int bx, int gx) {
     EGG_SKIP_IF_UNCHANGED(w.ctrl);
     const int M = w.ctrl[kCtrlM];
-    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o <= g.n_outer; o += gridDim.x * blockDim.x)
+    for (int o = bx * blockDim.x + threadIdx.x; o <= g.n_outer; o += gx * blockDim.x)
         w.outer_begin[o] = lower_bound_i(w.cell_outer, 0, M, o);
 }
 
@@ -313,32 +331,10 @@ __global__ void k_outer_ranges(Geom g, Work w) {
 // per-cell sums of sin(delta) and 1 - cos(delta), delta = x - cell corner,
 // plus the tight bounding box of each cell's points
 // ---------------------------------------------------------------------------
-namespace {
-
-struct TwoSum {
-    float hi, lo;
-};
-
-__device__ __forceinline__ TwoSum ts_add(TwoSum a, TwoSum b) {
-    float s = __fadd_rn(a.hi, b.hi);
-    float bb = __fsub_rn(s, a.hi);
-    float err = __fadd_rn(__fsub_rn(a.hi, __fsub_rn(s, bb)), __fsub_rn(b.hi, bb));
-    return {s, __fadd_rn(__fadd_rn(a.lo, b.lo), err)};
-}
-
-// warp-partial layout: ((field * d + l) * 2 + rec) * warps + warp, field in
-// {sum sin, sum 1-cos, min, max}, rec 0 = segment holding lane 0, 1 = lane 31
-__device__ __forceinline__ size_t wp_idx(int field, int l, int d, int rec, int nw, int warp) {
-    return ((size_t)(field * d + l) * 2 + rec) * nw + warp;
-}
-
-}  // namespace
-
 template <int D>
-__global__ void __launch_bounds__(256) k_cell_sums(Geom g, Work w) {
-    constexpr int DM = D > 0 ? D : kMaxDims;
+__device__ __forceinline__ void cell_sums_body(const Geom& g, const Work& w, int bx) {
     const int d = D > 0 ? D : g.d;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = bx * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     const int warp = i >> 5;
     const int nw = (g.n + 31) >> 5;
@@ -346,10 +342,7 @@ __global__ void __launch_bounds__(256) k_cell_sums(Geom g, Work w) {
     const bool valid = i < g.n;
     const int c = valid ? w.cell_of[i] : 0x7fffffff - lane;
     const int cnext = __shfl_down_sync(0xffffffffu, c, 1);
-    const int cprev = __shfl_up_sync(0xffffffffu, c, 1);
     const bool seg_end = valid && (lane == 31 || cnext != c);
-    const bool seg_start = valid && (lane == 0 || cprev != c);
-    (void)seg_start;
     const int wb = i & ~31;
     int cs = 0, ce = 0;
     if (seg_end) {
@@ -402,9 +395,8 @@ __global__ void __launch_bounds__(256) k_cell_sums(Geom g, Work w) {
             // partial of a cell spanning several warps: rec 0 = segment holding
             // lane 0 (continues from the previous warp), rec 1 = segment holding
             // lane 31 (continues into the next warp); a warp inside one cell
-            // writes both.
-            // The FP32 copy (gpart) is the record of this 32-point group of
-            // the cell, used by the update to decide groups wholesale.
+            // writes both.  The FP32 copy (gpart) is the record of this
+            // 32-point group of the cell, used to decide groups wholesale.
             const double S = (double)vs.hi + (double)vs.lo;
             const double Mm = (double)vm.hi + (double)vm.lo;
             const float Sf = __fadd_rn(vs.hi, vs.lo), Mf = __fadd_rn(vm.hi, vm.lo);
@@ -421,7 +413,6 @@ __global__ void __launch_bounds__(256) k_cell_sums(Geom g, Work w) {
             }
         }
     }
-    (void)DM;
 }
 
 // one big spanning cell, the whole warp: lanes stride over its warp partials
@@ -429,61 +420,59 @@ template <int D>
 __device__ void combine_big(const Geom& g, const Work& w, int c, int wh, int wt, int lane, int nw) {
     constexpr int DM = D > 0 ? D : 1;
     const int d = D > 0 ? D : g.d;
-    {
-        if (D > 0) {
-            // every dimension in one pass: 4*D independent loads per partial
-            double S[DM], Mm[DM], mn[DM], mx[DM];
+    if (D > 0) {
+        // every dimension in one pass: 4*D independent loads per partial
+        double S[DM], Mm[DM], mn[DM], mx[DM];
 #pragma unroll
-            for (int l = 0; l < DM; l++) { S[l] = 0.0; Mm[l] = 0.0; mn[l] = 1e300; mx[l] = -1e300; }
-            for (int k = wh + lane; k <= wt; k += 32) {
-                const int rec = (k == wh) ? 1 : 0;
-#pragma unroll
-                for (int l = 0; l < DM; l++) {
-                    S[l] += w.wpart[wp_idx(0, l, d, rec, nw, k)];
-                    Mm[l] += w.wpart[wp_idx(1, l, d, rec, nw, k)];
-                    mn[l] = fmin(mn[l], w.wpart[wp_idx(2, l, d, rec, nw, k)]);
-                    mx[l] = fmax(mx[l], w.wpart[wp_idx(3, l, d, rec, nw, k)]);
-                }
-            }
+        for (int l = 0; l < DM; l++) { S[l] = 0.0; Mm[l] = 0.0; mn[l] = 1e300; mx[l] = -1e300; }
+        for (int k = wh + lane; k <= wt; k += 32) {
+            const int rec = (k == wh) ? 1 : 0;
 #pragma unroll
             for (int l = 0; l < DM; l++) {
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    S[l] += __shfl_xor_sync(0xffffffffu, S[l], o);
-                    Mm[l] += __shfl_xor_sync(0xffffffffu, Mm[l], o);
-                    mn[l] = fmin(mn[l], __shfl_xor_sync(0xffffffffu, mn[l], o));
-                    mx[l] = fmax(mx[l], __shfl_xor_sync(0xffffffffu, mx[l], o));
-                }
-                if (lane == 0) {
-                    w.css[(size_t)l * g.ns + c] = (float)S[l];
-                    w.csm[(size_t)l * g.ns + c] = (float)Mm[l];
-                    w.cbmin[(size_t)l * g.ns + c] = (float)mn[l];
-                    w.cbmax[(size_t)l * g.ns + c] = (float)mx[l];
-                }
+                S[l] += w.wpart[wp_idx(0, l, d, rec, nw, k)];
+                Mm[l] += w.wpart[wp_idx(1, l, d, rec, nw, k)];
+                mn[l] = fmin(mn[l], w.wpart[wp_idx(2, l, d, rec, nw, k)]);
+                mx[l] = fmax(mx[l], w.wpart[wp_idx(3, l, d, rec, nw, k)]);
             }
-        } else {
-            for (int l = 0; l < d; l++) {
-                double S = 0.0, Mm = 0.0, mn = 1e300, mx = -1e300;
-                for (int k = wh + lane; k <= wt; k += 32) {
-                    const int rec = (k == wh) ? 1 : 0;
-                    S += w.wpart[wp_idx(0, l, d, rec, nw, k)];
-                    Mm += w.wpart[wp_idx(1, l, d, rec, nw, k)];
-                    mn = fmin(mn, w.wpart[wp_idx(2, l, d, rec, nw, k)]);
-                    mx = fmax(mx, w.wpart[wp_idx(3, l, d, rec, nw, k)]);
-                }
+        }
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    S += __shfl_xor_sync(0xffffffffu, S, o);
-                    Mm += __shfl_xor_sync(0xffffffffu, Mm, o);
-                    mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-                    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-                }
-                if (lane == 0) {
-                    w.css[(size_t)l * g.ns + c] = (float)S;
-                    w.csm[(size_t)l * g.ns + c] = (float)Mm;
-                    w.cbmin[(size_t)l * g.ns + c] = (float)mn;
-                    w.cbmax[(size_t)l * g.ns + c] = (float)mx;
-                }
+        for (int l = 0; l < DM; l++) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                S[l] += __shfl_xor_sync(0xffffffffu, S[l], o);
+                Mm[l] += __shfl_xor_sync(0xffffffffu, Mm[l], o);
+                mn[l] = fmin(mn[l], __shfl_xor_sync(0xffffffffu, mn[l], o));
+                mx[l] = fmax(mx[l], __shfl_xor_sync(0xffffffffu, mx[l], o));
+            }
+            if (lane == 0) {
+                w.css[(size_t)l * g.ns + c] = (float)S[l];
+                w.csm[(size_t)l * g.ns + c] = (float)Mm[l];
+                w.cbmin[(size_t)l * g.ns + c] = (float)mn[l];
+                w.cbmax[(size_t)l * g.ns + c] = (float)mx[l];
+            }
+        }
+    } else {
+        for (int l = 0; l < d; l++) {
+            double S = 0.0, Mm = 0.0, mn = 1e300, mx = -1e300;
+            for (int k = wh + lane; k <= wt; k += 32) {
+                const int rec = (k == wh) ? 1 : 0;
+                S += w.wpart[wp_idx(0, l, d, rec, nw, k)];
+                Mm += w.wpart[wp_idx(1, l, d, rec, nw, k)];
+                mn = fmin(mn, w.wpart[wp_idx(2, l, d, rec, nw, k)]);
+                mx = fmax(mx, w.wpart[wp_idx(3, l, d, rec, nw, k)]);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                S += __shfl_xor_sync(0xffffffffu, S, o);
+                Mm += __shfl_xor_sync(0xffffffffu, Mm, o);
+                mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+                mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            }
+            if (lane == 0) {
+                w.css[(size_t)l * g.ns + c] = (float)S;
+                w.csm[(size_t)l * g.ns + c] = (float)Mm;
+                w.cbmin[(size_t)l * g.ns + c] = (float)mn;
+                w.cbmax[(size_t)l * g.ns + c] = (float)mx;
             }
         }
     }
@@ -495,18 +484,18 @@ __device__ void combine_big(const Geom& g, const Work& w, int c, int wh, int wt,
 // boundary) a thread each.  The list order depends on scheduling, the result
 // of every cell does not.
 template <int D>
-__global__ void __launch_bounds__(256) k_cell_sums_fix(Geom g, Work w) {
+__device__ __forceinline__ void cell_sums_fix_body(const Geom& g, const Work& w, int bx, int gx) {
     const int d = D > 0 ? D : g.d;
     const int lane = threadIdx.x & 31;
     const int nw = (g.n + 31) >> 5;
     const int big = w.ctrl[kCtrlBigCount];
-    const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < big; e += warps) {
+    const int warps = (gx * blockDim.x) >> 5;
+    for (int e = (bx * blockDim.x + threadIdx.x) >> 5; e < big; e += warps) {
         const int c = w.big_list[e];
         combine_big<D>(g, w, c, w.cell_start[c] >> 5, (w.cell_start[c + 1] - 1) >> 5, lane, nw);
     }
     const int count = w.ctrl[kCtrlSpanCount];
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {
+    for (int e = bx * blockDim.x + threadIdx.x; e < count; e += gx * blockDim.x) {
         const int c = w.span_list[e];
         const int wh = w.cell_start[c] >> 5, wt = (w.cell_start[c + 1] - 1) >> 5;
         for (int l = 0; l < d; l++) {
@@ -524,6 +513,75 @@ __global__ void __launch_bounds__(256) k_cell_sums_fix(Geom g, Work w) {
             w.cbmax[(size_t)l * g.ns + c] = (float)mx;
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// single-instance and batched wrappers
+// ---------------------------------------------------------------------------
+#define EGG_WRAP0(NAME, BOUNDS, BODYCALL)                                            \
+    __global__ void __launch_bounds__(BOUNDS) k_##NAME(Geom g, Work w) {             \
+        const int bx = blockIdx.x, gx = gridDim.x;                                   \
+        (void)bx; (void)gx;                                                          \
+        BODYCALL;                                                                    \
+    }                                                                                \
+    __global__ void __launch_bounds__(BOUNDS) kb_##NAME(BatchArgs B, int skip) {     \
+        EGG_BATCH_ENTRY(B, skip);                                                    \
+        (void)bx; (void)gx;                                                          \
+        BODYCALL;                                                                    \
+    }
+
+#define EGG_WRAPD(NAME, BOUNDS, BODYCALL)                                                \
+    template <int D>                                                                     \
+    __global__ void __launch_bounds__(BOUNDS) k_##NAME(Geom g, Work w) {                 \
+        const int bx = blockIdx.x, gx = gridDim.x;                                       \
+        (void)bx; (void)gx;                                                              \
+        BODYCALL;                                                                        \
+    }                                                                                    \
+    template <int D>                                                                     \
+    __global__ void __launch_bounds__(BOUNDS) kb_##NAME(BatchArgs B, int skip) {         \
+        EGG_BATCH_ENTRY(B, skip);                                                        \
+        (void)bx; (void)gx;                                                              \
+        BODYCALL;                                                                        \
+    }
+
+EGG_WRAPD(check_cells, 256, check_cells_body<D>(g, w, bx, gx))
+EGG_WRAP0(build_begin, 32, (void)g; if (threadIdx.x == 0) build_begin_body(w))
+EGG_WRAP0(scan_block_sums, 1024, scan_block_sums_body(g, w))
+EGG_WRAP0(radix_scan, 256, radix_scan_body(g, w, bx))
+EGG_WRAPD(heads_finalize, kHeadsBlock, heads_finalize_body<D>(g, w, bx))
+EGG_WRAP0(outer_ranges, 256, outer_ranges_body(g, w, bx, gx))
+EGG_WRAPD(cell_sums, 256, cell_sums_body<D>(g, w, bx))
+EGG_WRAPD(cell_sums_fix, 256, cell_sums_fix_body<D>(g, w, bx, gx))
+
+__global__ void __launch_bounds__(kSortThreads) k_radix_hist(Geom g, Work w, int in_sel, int first, int dim,
+                                                             int shift) {
+    radix_hist_body(g, w, in_sel, first, dim, shift, blockIdx.x);
+}
+__global__ void __launch_bounds__(kSortThreads) kb_radix_hist(BatchArgs B, int skip, int in_sel, int first, int dim,
+                                                              int shift) {
+    EGG_BATCH_ENTRY(B, skip);
+    (void)gx;
+    radix_hist_body(g, w, in_sel, first, dim, shift, bx);
+}
+__global__ void __launch_bounds__(kSortThreads) k_radix_scatter(Geom g, Work w, int in_sel, int out_sel, int first,
+                                                                int dim, int shift) {
+    radix_scatter_body(g, w, in_sel, out_sel, first, dim, shift, blockIdx.x);
+}
+__global__ void __launch_bounds__(kSortThreads) kb_radix_scatter(BatchArgs B, int skip, int in_sel, int out_sel,
+                                                                 int first, int dim, int shift) {
+    EGG_BATCH_ENTRY(B, skip);
+    (void)gx;
+    radix_scatter_body(g, w, in_sel, out_sel, first, dim, shift, bx);
+}
+template <int D>
+__global__ void __launch_bounds__(kHeadsBlock) k_gather_heads(Geom g, Work w, int identity) {
+    gather_heads_body<D>(g, w, identity, blockIdx.x);
+}
+template <int D>
+__global__ void __launch_bounds__(kHeadsBlock) kb_gather_heads(BatchArgs B, int skip, int identity) {
+    EGG_BATCH_ENTRY(B, skip);
+    (void)gx;
+    gather_heads_body<D>(g, w, identity, bx);
 }
 
 // ---------------------------------------------------------------------------
@@ -582,47 +640,49 @@ __global__ void k_unsort_int(Geom g, Work w, const int* __restrict__ src, int* _
         default: KERNEL<0> __VA_ARGS__; break;        \
     }
 
-void launch_sort(const Geom& g, const Work& w, const SortPlan& plan, cudaStream_t st) {
-    const int tiles = (g.n + kSortTile - 1) / kSortTile;
-    const int* pin = nullptr;
-    int* bufs[2] = {w.perm, w.perm_tmp};
-    // the last pass must land in w.perm
+// launch NAME (plain) or its batched twin with the same extra arguments
+#define EGG_GO(ex, shape, threads, st, NAME, ...)                                                     \
+    do {                                                                                             \
+        if ((ex).batch())                                                                            \
+            kb_##NAME<<<(ex).blocks(shape), threads, 0, st>>>((ex).args(shape), (ex).skip_done, ##__VA_ARGS__); \
+        else                                                                                         \
+            k_##NAME<<<(ex).blocks(shape), threads, 0, st>>>(*(ex).g, *(ex).w, ##__VA_ARGS__);       \
+    } while (0)
+
+#define EGG_GO_D(ex, shape, threads, st, NAME, ...)                                                   \
+    do {                                                                                             \
+        if ((ex).batch()) {                                                                          \
+            EGG_DISPATCH_D((ex).d, kb_##NAME,                                                        \
+                           <<<(ex).blocks(shape), threads, 0, st>>>((ex).args(shape), (ex).skip_done, ##__VA_ARGS__)); \
+        } else {                                                                                     \
+            EGG_DISPATCH_D((ex).d, k_##NAME, <<<(ex).blocks(shape), threads, 0, st>>>(*(ex).g, *(ex).w, ##__VA_ARGS__)); \
+        }                                                                                            \
+    } while (0)
+
+void launch_build(const Exec& ex, const SortPlan& plan, cudaStream_t st) {
+    EGG_GO(ex, kShapeOne, 32, st, build_begin);
+    EGG_GO_D(ex, kShapeCapN256, 256, st, check_cells);
+    // radix passes; the last one must land in perm (selector 0)
     int out = (plan.count % 2 == 1) ? 0 : 1;
+    int in = 0;
     for (int p = 0; p < plan.count; p++) {
         const int first = (p == 0);
-        int* pout = bufs[out];
-        k_radix_hist<<<tiles, kSortThreads, 0, st>>>(g, w.Xn, pin, first, plan.dim[p], plan.shift[p], w.hist, tiles,
-                                                     w.ctrl);
-        k_radix_scan<<<256, 256, 0, st>>>(w.hist, tiles, w.digit_total, w.ctrl);
-        k_radix_scatter<<<tiles, kSortThreads, 0, st>>>(g, w.Xn, pin, first, plan.dim[p], plan.shift[p], w.hist,
-                                                        w.digit_total, tiles, pout, w.ctrl);
-        pin = pout;
+        EGG_GO(ex, kShapeTiles, kSortThreads, st, radix_hist, in, first, plan.dim[p], plan.shift[p]);
+        EGG_GO(ex, kShapeDigits, 256, st, radix_scan);
+        EGG_GO(ex, kShapeTiles, kSortThreads, st, radix_scatter, in, out, first, plan.dim[p], plan.shift[p]);
+        in = out;
         out ^= 1;
     }
-}
-
-void launch_build(const Geom& g, const Work& w, const SortPlan& plan, cudaStream_t st) {
-    {
-        k_build_begin<<<1, 1, 0, st>>>(w.ctrl);
-        int blocks = (g.n + 255) / 256;
-        if (blocks > 148 * 8) blocks = 148 * 8;
-        EGG_DISPATCH_D(g.d, k_check_cells, <<<blocks, 256, 0, st>>>(g, w));
-    }
     const int identity = plan.count == 0;
-    if (!identity) launch_sort(g, w, plan, st);
-    const int nb = (g.n + kHeadsBlock - 1) / kHeadsBlock;
-    EGG_DISPATCH_D(g.d, k_gather_heads, <<<nb, kHeadsBlock, 0, st>>>(g, w, identity));
-    k_scan_block_sums<<<1, 1024, 0, st>>>(w.block_sums, nb, w.ctrl);
-    EGG_DISPATCH_D(g.d, k_heads_finalize, <<<nb, kHeadsBlock, 0, st>>>(g, w));
-    k_outer_ranges<<<(g.n_outer + 1 + 255) / 256, 256, 0, st>>>(g, w);
+    EGG_GO_D(ex, kShapeN1024, kHeadsBlock, st, gather_heads, identity);
+    EGG_GO(ex, kShapeOne, 1024, st, scan_block_sums);
+    EGG_GO_D(ex, kShapeN1024, kHeadsBlock, st, heads_finalize);
+    EGG_GO(ex, kShapeOuter, 256, st, outer_ranges);
 }
 
-void launch_cell_sums(const Geom& g, const Work& w, cudaStream_t st) {
-    const int blocks = (g.n + 255) / 256;
-    EGG_DISPATCH_D(g.d, k_cell_sums, <<<blocks, 256, 0, st>>>(g, w));
-    int fix_blocks = ((g.n + 31) / 32 + 7) / 8;  // one warp per possible spanning cell
-    if (fix_blocks > 148 * 8) fix_blocks = 148 * 8;
-    EGG_DISPATCH_D(g.d, k_cell_sums_fix, <<<fix_blocks, 256, 0, st>>>(g, w));
+void launch_cell_sums(const Exec& ex, cudaStream_t st) {
+    EGG_GO_D(ex, kShapeN256, 256, st, cell_sums);
+    EGG_GO_D(ex, kShapeFix, 256, st, cell_sums_fix);
 }
 
 void launch_transpose_in(const Geom& g, const Work& w, const float* x, cudaStream_t st) {

@@ -379,19 +379,19 @@ void enqueue_iteration(Instance& I, cudaGraphConditionalHandle h, int in_graph, 
     };
     k_iter_begin<<<1, 1, 0, st>>>(I.w);
     mark(0);
-    launch_build(I.g, I.w, I.plan, st);
+    launch_build(single(I.g, I.w), I.plan, st);
     mark(1);
     mark(2);
-    launch_cell_sums(I.g, I.w, st);
-    launch_need(I.g, I.w, st);
+    launch_cell_sums(single(I.g, I.w), st);
+    launch_need(single(I.g, I.w), st);
     if (I.g.order_mode == 2 || I.g.stop_rule == 1) launch_order_param(I.g, I.w, -1, st);
     mark(3);
     mark(4);
-    launch_update(I.g, I.w, nullptr, st);
+    launch_update(single(I.g, I.w), nullptr, st);
     mark(5);
     k_mark_extra<<<1, 1, 0, st>>>(I.w);
     mark(6);
-    launch_extra_check(I.g, I.w, st);
+    launch_extra_check(single(I.g, I.w), st);
     mark(7);
     k_iter_end<<<1, 1, 0, st>>>(I.w, h, in_graph, I.g.stop_rule);
 }
@@ -554,14 +554,14 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
     }
     EGG_CHECK(cudaEventRecord(I.ev[2], I.st));
     // final grid and labels (EGG_SynC.cu:1503-1522)
-    launch_build(I.g, I.w, I.plan, I.st);
+    launch_build(single(I.g, I.w), I.plan, I.st);
     const bool dev_out = is_device_ptr(labels);
     int* lab = dev_out ? labels : I.w.labels;
     if (opts.labels_mode == 1) launch_labels(I.g, I.w, lab, I.st);
     else launch_labels_uf(I.g, I.w, lab, I.st);
     if (g.order_mode == 1) {
         // the final positions' order parameter needs their cell sums
-        launch_cell_sums(I.g, I.w, I.st);
+        launch_cell_sums(single(I.g, I.w), I.st);
         launch_order_param(I.g, I.w, max_iter + 1, I.st);
     }
     if (opts.positions_out) {
@@ -659,15 +659,15 @@ int step(const float* x, int64_t n, int32_t d, float eps, float* x_next, int32_t
     check_status_bits(I);
     cudaStream_t st = I.st;
     k_iter_begin<<<1, 1, 0, st>>>(I.w);
-    launch_build(I.g, I.w, I.plan, st);
-    launch_cell_sums(I.g, I.w, st);
-    launch_need(I.g, I.w, st);
+    launch_build(single(I.g, I.w), I.plan, st);
+    launch_cell_sums(single(I.g, I.w), st);
+    launch_need(single(I.g, I.w), st);
     int* cnt_sorted = I.w.orig_tmp;  // free once the grid is built
-    launch_update(I.g, I.w, cnt_sorted, st);
+    launch_update(single(I.g, I.w), cnt_sorted, st);
     EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, kCtrlWords * sizeof(int), cudaMemcpyDeviceToHost, st));
     EGG_CHECK(cudaStreamSynchronize(st));
     flags[0] = I.h_ctrl[kCtrlFlag];
-    launch_extra_check(I.g, I.w, st);
+    launch_extra_check(single(I.g, I.w), st);
     EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, kCtrlWords * sizeof(int), cudaMemcpyDeviceToHost, st));
     // updated positions back to the original order (staged in qlo, free now)
     const bool dev_x = is_device_ptr(x_next);
@@ -697,7 +697,7 @@ int grid(const float* x, int64_t n, int32_t d, float eps, int32_t* order, int32_
     prepare(I, g, 4);
     load_input(I, x);
     check_status_bits(I);
-    launch_build(I.g, I.w, I.plan, I.st);
+    launch_build(single(I.g, I.w), I.plan, I.st);
     EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, kCtrlWords * sizeof(int), cudaMemcpyDeviceToHost, I.st));
     EGG_CHECK(cudaStreamSynchronize(I.st));
     const int M = I.h_ctrl[kCtrlM];
@@ -804,7 +804,7 @@ int grid_noalloc(const float* x, int64_t n, int32_t d, float eps, int32_t* order
         src = xin;
     }
     launch_transpose_in(g, w, src, st);
-    launch_build(g, w, plan, st);
+    launch_build(single(g, w), plan, st);
     int ctrl_h[kCtrlWords];
     EGG_CHECK(cudaMemcpyAsync(ctrl_h, w.ctrl, sizeof(ctrl_h), cudaMemcpyDeviceToHost, st));
     EGG_CHECK(cudaStreamSynchronize(st));

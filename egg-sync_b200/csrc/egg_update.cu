@@ -198,18 +198,18 @@ __device__ __forceinline__ void visit_cell(const Geom& g, const Work& w, int c, 
 // walks the stencil on its own.  Both paths visit a superset of the cells
 // the reference visits and apply the reference's per-point box test to each.
 template <int D>
-__global__ void __launch_bounds__(128) k_update(Geom g, Work w, int* __restrict__ counts) {
+__device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* __restrict__ counts, int bx) {
     constexpr int DM = D > 0 ? D : kMaxDims;
     const int d = D > 0 ? D : g.d;
     extern __shared__ float s_tab[];
     const int K = g.table_k, TW = 2 * K + 1;
     for (int t = threadIdx.x; t < 3 * TW; t += blockDim.x) s_tab[t] = w.table[t];
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (bx == 0 && threadIdx.x == 0) {
         const int it = w.ctrl[kCtrlIter];
         w.stamps[4 * it + 1] = globaltimer();
     }
     __syncthreads();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = bx * blockDim.x + threadIdx.x;
     if ((i & ~31) >= g.n) return;  // whole warp beyond n
     const int lane = threadIdx.x & 31;
     const bool valid = i < g.n;
@@ -307,6 +307,18 @@ __global__ void __launch_bounds__(128) k_update(Geom g, Work w, int* __restrict_
     if (a.tab_err) atomicOr(w.ctrl + kCtrlStatus, kErrTable);
 }
 
+template <int D>
+__global__ void __launch_bounds__(128) k_update(Geom g, Work w, int* __restrict__ counts) {
+    update_body<D>(g, w, counts, blockIdx.x);
+}
+
+template <int D>
+__global__ void __launch_bounds__(128) kb_update(BatchArgs B, int skip) {
+    EGG_BATCH_ENTRY(B, skip);
+    (void)gx;
+    update_body<D>(g, w, nullptr, bx);
+}
+
 #define EGG_DISPATCH_D(d, KERNEL, ...)                \
     switch (d) {                                      \
         case 1: KERNEL<1> __VA_ARGS__; break;         \
@@ -324,11 +336,11 @@ __global__ void __launch_bounds__(128) k_update(Geom g, Work w, int* __restrict_
 // stencil of every outer cell that the previous update marked dirty (a moved
 // point's old or new position); the marks are cleared as they are consumed,
 // so the array is clean again when the update after next writes it.
-__global__ void k_need(Geom g, Work w) {
+__device__ __forceinline__ void need_body(const Geom& g, const Work& w, int bx, int gx) {
     const int it = w.ctrl[kCtrlIter];
     unsigned char* prev = w.dirty[(it + 1) & 1];
     const int nst = w.st_count[0];
-    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < g.n_outer; o += gridDim.x * blockDim.x) {
+    for (int o = bx * blockDim.x + threadIdx.x; o < g.n_outer; o += gx * blockDim.x) {
         if (!prev[o]) continue;
         prev[o] = 0;
         int co[32];
@@ -348,17 +360,29 @@ __global__ void k_need(Geom g, Work w) {
     }
 }
 
-void launch_need(const Geom& g, const Work& w, cudaStream_t st) {
-    int blocks = (g.n_outer + 255) / 256;
-    if (blocks > 148 * 8) blocks = 148 * 8;
-    k_need<<<blocks, 256, 0, st>>>(g, w);
+__global__ void k_need(Geom g, Work w) { need_body(g, w, blockIdx.x, gridDim.x); }
+
+__global__ void kb_need(BatchArgs B, int skip) {
+    EGG_BATCH_ENTRY(B, skip);
+    need_body(g, w, bx, gx);
 }
 
-void launch_update(const Geom& g, const Work& w, int* counts, cudaStream_t st) {
+void launch_need(const Exec& ex, cudaStream_t st) {
+    if (ex.batch())
+        kb_need<<<ex.blocks(kShapeCapOuter), 256, 0, st>>>(ex.args(kShapeCapOuter), ex.skip_done);
+    else
+        k_need<<<ex.blocks(kShapeCapOuter), 256, 0, st>>>(*ex.g, *ex.w);
+}
+
+void launch_update(const Exec& ex, int* counts, cudaStream_t st) {
     const int threads = 128;
-    const int blocks = (g.n + threads - 1) / threads;
-    const size_t smem = sizeof(float) * 3 * (2 * g.table_k + 1);
-    EGG_DISPATCH_D(g.d, k_update, <<<blocks, threads, smem, st>>>(g, w, counts));
+    const size_t smem = sizeof(float) * 3 * (2 * ex.table_k() + 1);
+    if (ex.batch()) {
+        EGG_DISPATCH_D(ex.d, kb_update,
+                       <<<ex.blocks(kShapeN128), threads, smem, st>>>(ex.args(kShapeN128), ex.skip_done));
+    } else {
+        EGG_DISPATCH_D(ex.d, k_update, <<<ex.blocks(kShapeN128), threads, smem, st>>>(*ex.g, *ex.w, counts));
+    }
 }
 
 }  // namespace egg
