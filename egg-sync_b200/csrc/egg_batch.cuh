@@ -1,16 +1,23 @@
 // egg_batch.cuh -- one launch for many instances.
 //
-// Every per-iteration kernel is written as a device body taking its block
-// index bx and block count gx.  The single-instance kernel calls it with
-// (blockIdx.x, gridDim.x); the batched kernel maps blockIdx.x to (instance,
-// local block) through a prefix table of per-instance block counts and runs
-// the same body on that instance's geometry and workspace, copied to shared
-// memory.  Blocks of instances whose loop has finished return at once.
+// Every per-iteration kernel is written as a device body over a block index
+// bx of gx blocks.  The single-instance kernel calls it with (blockIdx.x,
+// gridDim.x).  The batched kernel is persistent: its blocks stride over the
+// virtual blocks of all instances still in the active list (for a launch
+// shape s, instance k of the list owns virtual blocks [boff[k], boff[k+1])),
+// copy that instance's geometry and workspace descriptor to shared memory and
+// run the same body.  The active list and its offset tables are rebuilt on
+// the device after every iteration, so the cost of a launch follows the
+// instances that still iterate, and one CUDA graph replays the loop of the
+// whole batch.
 #pragma once
 
 #include "egg_common.cuh"
 
 namespace egg {
+
+constexpr int kScanSmallTiles = 64;  // radix digit scan: one block per instance up to this many tiles
+constexpr int kMaxBatch = 1024;      // instances of one batched call
 
 // launch shapes: how many blocks a kernel uses for one instance
 enum Shape : int {
@@ -18,7 +25,7 @@ enum Shape : int {
     kShapeN256,        // ceil(n / 256)
     kShapeN1024,       // ceil(n / 1024)
     kShapeTiles,       // ceil(n / kSortTile)
-    kShapeDigits,      // 256
+    kShapeDigits,      // 1 (few tiles: one thread per digit) or 256 (one block per digit)
     kShapeOne,         // 1
     kShapeOuter,       // ceil((n_outer + 1) / 256)
     kShapeCapN256,     // min(ceil(n / 256), 148 * 8)
@@ -26,8 +33,11 @@ enum Shape : int {
     kShapeCapOuter,    // min(ceil(n_outer / 256), 148 * 8)
     kShapeFix,         // min(ceil(ceil(n / 32) / 8), 148 * 8)
     kShapeCapN256L,    // min(ceil(n / 256), 148 * 16)
+    kShapeN64,         // ceil(n / 64)
     kShapeCount
 };
+
+__host__ __device__ inline int sort_tiles(const Geom& g) { return (g.n + kSortTile - 1) / kSortTile; }
 
 __host__ __device__ inline int shape_blocks(int shape, const Geom& g) {
     auto cdiv = [](long a, long b) { return (int)((a + b - 1) / b); };
@@ -36,8 +46,8 @@ __host__ __device__ inline int shape_blocks(int shape, const Geom& g) {
         case kShapeN128: return cdiv(g.n, 128);
         case kShapeN256: return cdiv(g.n, 256);
         case kShapeN1024: return cdiv(g.n, kHeadsBlock);
-        case kShapeTiles: return cdiv(g.n, kSortTile);
-        case kShapeDigits: return 256;
+        case kShapeTiles: return sort_tiles(g);
+        case kShapeDigits: return sort_tiles(g) <= kScanSmallTiles ? 1 : 256;
         case kShapeOne: return 1;
         case kShapeOuter: return cdiv((long)g.n_outer + 1, 256);
         case kShapeCapN256: return cap(cdiv(g.n, 256), 148 * 8);
@@ -45,39 +55,84 @@ __host__ __device__ inline int shape_blocks(int shape, const Geom& g) {
         case kShapeCapOuter: return cap(cdiv(g.n_outer, 256) > 0 ? cdiv(g.n_outer, 256) : 1, 148 * 8);
         case kShapeFix: return cap(cdiv(cdiv(g.n, 32), 8), 148 * 8);
         case kShapeCapN256L: return cap(cdiv(g.n, 256), 148 * 16);
+        case kShapeN64: return cdiv(g.n, 64);
         default: return 1;
     }
 }
 
+// Radix passes of an instance, least significant first: the sub-cell key,
+// then g_{d-1}, ..., g_od, then g_0, ..., g_{od-1}; two 8-bit passes per
+// dimension when there are more than 256 cells per dimension.  The last
+// pass must write perm (selector 0); pass p reads what pass p-1 wrote.
+__host__ __device__ inline int plan_count(const Geom& g) { return 1 + g.d * (g.width > 256 ? 2 : 1); }
+
+__host__ __device__ inline void plan_pass(const Geom& g, int p, int& dim, int& shift) {
+    if (p == 0) {
+        dim = -1;
+        shift = 0;
+        return;
+    }
+    const int per = g.width > 256 ? 2 : 1;
+    const int k = (p - 1) / per;
+    const int nin = g.d - g.od;
+    dim = k < nin ? g.d - 1 - k : k - nin;
+    shift = 8 * ((p - 1) % per);
+}
+
+__host__ __device__ inline int plan_out_sel(int count, int p) { return ((count - p) & 1) ? 0 : 1; }
+
 struct BatchArgs {
-    const Geom* geoms;  // [ninst]
-    const Work* works;  // [ninst]
-    const int* boff;    // [ninst + 1] block offsets of this launch's shape
-    int ninst;
+    const Geom* geoms;   // [instances]
+    const Work* works;   // [instances]
+    const int* boff;     // [list + 1] virtual-block offsets of this launch's shape
+    const int* active;   // [list] instance ids
+    const int* nact;     // list length
 };
 
-// Declares `g`, `w`, `bx`, `gx` for the block's instance (shared-memory
-// copies) and returns for instances whose loop is done when skip_done.
-#define EGG_BATCH_ENTRY(B, skip_done)                                                          \
-    __shared__ Geom _bg;                                                                       \
-    __shared__ Work _bw;                                                                       \
-    __shared__ int _bbx, _bgx, _bskip;                                                         \
-    if (threadIdx.x == 0) {                                                                    \
-        int lo_ = 0, hi_ = (B).ninst - 1;                                                      \
-        while (lo_ < hi_) {                                                                    \
-            const int m_ = (lo_ + hi_ + 1) >> 1;                                               \
-            if ((B).boff[m_] <= (int)blockIdx.x) lo_ = m_; else hi_ = m_ - 1;                  \
-        }                                                                                      \
-        _bg = (B).geoms[lo_];                                                                  \
-        _bw = (B).works[lo_];                                                                  \
-        _bbx = (int)blockIdx.x - (B).boff[lo_];                                                \
-        _bgx = (B).boff[lo_ + 1] - (B).boff[lo_];                                              \
-        _bskip = (skip_done) && _bw.ctrl[kCtrlDone] != 0;                                      \
-    }                                                                                          \
-    __syncthreads();                                                                           \
-    if (_bskip) return;                                                                        \
-    const Geom& g = _bg;                                                                       \
-    const Work& w = _bw;                                                                       \
-    const int bx = _bbx, gx = _bgx;
+// Runs body(g, w, bx, gx) for every virtual block of the listed instances.
+// Virtual blocks are dealt out with stride gridDim.x, which spreads the
+// dense regions of every instance over all SMs.  Each block copies the
+// offset table to shared memory once and the descriptors of an instance only
+// when its next virtual block belongs to another instance.
+template <typename F>
+__device__ __forceinline__ void batch_for(const BatchArgs& B, F&& body) {
+    static_assert(sizeof(Geom) % 4 == 0 && sizeof(Work) % 4 == 0, "descriptor copy by words");
+    __shared__ Geom s_g;
+    __shared__ Work s_w;
+    __shared__ int s_boff[kMaxBatch + 1];
+    __shared__ int s_info[4];  // list entry, its first virtual block, its block count, entry loaded
+    const int na = *B.nact;
+    const int tot = B.boff[na];
+    if ((int)blockIdx.x >= tot) return;
+    for (int t = threadIdx.x; t <= na; t += blockDim.x) s_boff[t] = B.boff[t];
+    if (threadIdx.x == 0) s_info[3] = -1;
+    __syncthreads();
+    for (int vb = blockIdx.x; vb < tot; vb += gridDim.x) {
+        if (threadIdx.x == 0) {
+            int lo = 0, hi = na - 1;
+            while (lo < hi) {
+                const int m = (lo + hi + 1) >> 1;
+                if (s_boff[m] <= vb) lo = m; else hi = m - 1;
+            }
+            s_info[0] = lo;
+            s_info[1] = s_boff[lo];
+            s_info[2] = s_boff[lo + 1] - s_boff[lo];
+        }
+        __syncthreads();
+        if (s_info[0] != s_info[3]) {
+            const int inst = B.active[s_info[0]];
+            const int* sg = reinterpret_cast<const int*>(B.geoms + inst);
+            const int* sw = reinterpret_cast<const int*>(B.works + inst);
+            int* dg = reinterpret_cast<int*>(&s_g);
+            int* dw = reinterpret_cast<int*>(&s_w);
+            for (int t = threadIdx.x; t < (int)(sizeof(Geom) / 4); t += blockDim.x) dg[t] = sg[t];
+            for (int t = threadIdx.x; t < (int)(sizeof(Work) / 4); t += blockDim.x) dw[t] = sw[t];
+            __syncthreads();
+            if (threadIdx.x == 0) s_info[3] = s_info[0];
+        }
+        body(static_cast<const Geom&>(s_g), static_cast<const Work&>(s_w), vb - s_info[1], s_info[2]);
+        __syncthreads();
+    }
+}
 
 }  // namespace egg

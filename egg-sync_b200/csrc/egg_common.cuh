@@ -97,7 +97,7 @@ struct Work {
     unsigned long long* stamps;  // [max_iter+1] globaltimer at iteration start
     int* labels;       // [ns] output labels (original order)
     int* iter_flags;   // [max_iter] flag after each iteration
-    int* iter_counts;  // reserved
+    unsigned long long* ustats;  // [kUStats] interaction counters of the update kernel (stats build)
     // incremental update: outer cells touched by a moved point (old or new
     // position) in the last update, ping-pong by iteration parity; the
     // stencil dilation of those marks; the last violation bit of every point
@@ -112,6 +112,8 @@ struct Work {
     // union-find labelling
     int* uf_parent;            // [ns]
     int* uf_size;              // [ns]
+    // batched runs: this instance's input (device, row-major n x d)
+    const float* src;
 };
 
 enum : int {
@@ -134,6 +136,27 @@ enum : int {
     kCtrlBigCount = 16,   // cells over 4 or more warps listed in big_list
     kCtrlLamReached = 17, // the order parameter's lower bound reached lambda this iteration
     kCtrlWords = 32,      // size of the control-word array
+};
+
+// Interaction counters of the update kernel, summed over a run.  Collected
+// only in the stats build (EGG_UPDATE_STATS, libeggsync_stats.so); they give
+// the kernel's algorithmic work: cells examined and how each was decided,
+// point pairs tested.
+enum : int {
+    kUsPoints = 0,     // point updates computed
+    kUsCells,          // candidate cells examined (box test)
+    kUsSmallPass,      // ... passing the reference's small box test
+    kUsFull,           // ... fully covered (box), aggregated
+    kUsTightIn,        // ... all points within eps by their tight box, aggregated
+    kUsTightOut,       // ... no point within eps by their tight box, skipped
+    kUsGroupsIn,       // 32-point groups of spanning cells aggregated
+    kUsGroupsOut,      // 32-point groups skipped
+    kUsPairs,          // point-pair distance tests
+    kUsPairsIn,        // ... within eps
+    kUsLaneWarps,      // warps that walked the stencil lane by lane
+    kUsHalfCount,      // border points that needed the half count
+    kUsNeighbors,      // sum of |N(p)|
+    kUStats = 16
 };
 
 // ------------------------------------------------------------------------

@@ -235,21 +235,18 @@ __device__ __forceinline__ void annulus_body(const Geom& g, const Work& w, int b
 template <int D>
 __global__ void __launch_bounds__(128) k_ball_bbox(Geom g, Work w) { ball_bbox_body<D>(g, w, blockIdx.x, gridDim.x); }
 template <int D>
-__global__ void __launch_bounds__(128) kb_ball_bbox(BatchArgs B, int skip) {
-    EGG_BATCH_ENTRY(B, skip);
-    ball_bbox_body<D>(g, w, bx, gx);
+__global__ void __launch_bounds__(128) kb_ball_bbox(BatchArgs B) {
+    batch_for(B, [&](const Geom& g, const Work& w, int bx, int gx) { ball_bbox_body<D>(g, w, bx, gx); });
 }
 __global__ void __launch_bounds__(256) k_cell_ballbox(Geom g, Work w) { cell_ballbox_body(g, w, blockIdx.x, gridDim.x); }
-__global__ void __launch_bounds__(256) kb_cell_ballbox(BatchArgs B, int skip) {
-    EGG_BATCH_ENTRY(B, skip);
-    cell_ballbox_body(g, w, bx, gx);
+__global__ void __launch_bounds__(256) kb_cell_ballbox(BatchArgs B) {
+    batch_for(B, [&](const Geom& g, const Work& w, int bx, int gx) { cell_ballbox_body(g, w, bx, gx); });
 }
 template <int D>
 __global__ void __launch_bounds__(128) k_annulus(Geom g, Work w) { annulus_body<D>(g, w, blockIdx.x, gridDim.x); }
 template <int D>
-__global__ void __launch_bounds__(128) kb_annulus(BatchArgs B, int skip) {
-    EGG_BATCH_ENTRY(B, skip);
-    annulus_body<D>(g, w, bx, gx);
+__global__ void __launch_bounds__(128) kb_annulus(BatchArgs B) {
+    batch_for(B, [&](const Geom& g, const Work& w, int bx, int gx) { annulus_body<D>(g, w, bx, gx); });
 }
 
 #define EGG_DISPATCH_D(d, KERNEL, ...)                \
@@ -268,12 +265,12 @@ __global__ void __launch_bounds__(128) kb_annulus(BatchArgs B, int skip) {
 // Both kernels return at once unless the update left the flag at 1; the
 // grids are bounded so that the common early exit costs little.
 void launch_extra_check(const Exec& ex, cudaStream_t st) {
-    const int blocks = ex.blocks(kShapeCapN128);
+    const int blocks = ex.blocks(kShapeCapN128, 128);
     if (ex.batch()) {
         const BatchArgs B = ex.args(kShapeCapN128);
-        EGG_DISPATCH_D(ex.d, kb_ball_bbox, <<<blocks, 128, 0, st>>>(B, ex.skip_done));
-        kb_cell_ballbox<<<blocks, 256, 0, st>>>(B, ex.skip_done);
-        EGG_DISPATCH_D(ex.d, kb_annulus, <<<blocks, 128, 0, st>>>(B, ex.skip_done));
+        EGG_DISPATCH_D(ex.d, kb_ball_bbox, <<<blocks, 128, 0, st>>>(B));
+        kb_cell_ballbox<<<ex.blocks(kShapeCapN128, 256), 256, 0, st>>>(B);
+        EGG_DISPATCH_D(ex.d, kb_annulus, <<<blocks, 128, 0, st>>>(B));
     } else {
         EGG_DISPATCH_D(ex.d, k_ball_bbox, <<<blocks, 128, 0, st>>>(*ex.g, *ex.w));
         k_cell_ballbox<<<blocks, 256, 0, st>>>(*ex.g, *ex.w);

@@ -168,6 +168,21 @@ __device__ __forceinline__ void radix_hist_body(const Geom& g, const Work& w, in
 __device__ __forceinline__ void radix_scan_body(const Geom& g, const Work& w, int bx) {
     EGG_SKIP_IF_UNCHANGED(w.ctrl);
     const int tiles = (g.n + kSortTile - 1) / kSortTile;
+    if (tiles <= kScanSmallTiles) {
+        // one block for all digits: a thread walks its digit's tiles
+        const int t = threadIdx.x;
+        if (t < 256) {
+            int* h = w.hist + (size_t)t * tiles;
+            int run = 0;
+            for (int k = 0; k < tiles; k++) {
+                const int v = h[k];
+                h[k] = run;
+                run += v;
+            }
+            w.digit_total[t] = run;
+        }
+        return;
+    }
     int* h = w.hist + (size_t)bx * tiles;
     const int per = (tiles + blockDim.x - 1) / blockDim.x;
     const int b = threadIdx.x * per;
@@ -524,10 +539,11 @@ __device__ __forceinline__ void cell_sums_fix_body(const Geom& g, const Work& w,
         (void)bx; (void)gx;                                                          \
         BODYCALL;                                                                    \
     }                                                                                \
-    __global__ void __launch_bounds__(BOUNDS) kb_##NAME(BatchArgs B, int skip) {     \
-        EGG_BATCH_ENTRY(B, skip);                                                    \
-        (void)bx; (void)gx;                                                          \
-        BODYCALL;                                                                    \
+    __global__ void __launch_bounds__(BOUNDS) kb_##NAME(BatchArgs B) {               \
+        batch_for(B, [&](const Geom& g, const Work& w, int bx, int gx) {             \
+            (void)bx; (void)gx;                                                      \
+            BODYCALL;                                                                \
+        });                                                                          \
     }
 
 #define EGG_WRAPD(NAME, BOUNDS, BODYCALL)                                                \
@@ -538,16 +554,17 @@ __device__ __forceinline__ void cell_sums_fix_body(const Geom& g, const Work& w,
         BODYCALL;                                                                        \
     }                                                                                    \
     template <int D>                                                                     \
-    __global__ void __launch_bounds__(BOUNDS) kb_##NAME(BatchArgs B, int skip) {         \
-        EGG_BATCH_ENTRY(B, skip);                                                        \
-        (void)bx; (void)gx;                                                              \
-        BODYCALL;                                                                        \
+    __global__ void __launch_bounds__(BOUNDS) kb_##NAME(BatchArgs B) {                   \
+        batch_for(B, [&](const Geom& g, const Work& w, int bx, int gx) {                 \
+            (void)bx; (void)gx;                                                          \
+            BODYCALL;                                                                    \
+        });                                                                              \
     }
 
 EGG_WRAPD(check_cells, 256, check_cells_body<D>(g, w, bx, gx))
 EGG_WRAP0(build_begin, 32, (void)g; if (threadIdx.x == 0) build_begin_body(w))
 EGG_WRAP0(scan_block_sums, 1024, scan_block_sums_body(g, w))
-EGG_WRAP0(radix_scan, 256, radix_scan_body(g, w, bx))
+__global__ void __launch_bounds__(256) k_radix_scan(Geom g, Work w) { radix_scan_body(g, w, blockIdx.x); }
 EGG_WRAPD(heads_finalize, kHeadsBlock, heads_finalize_body<D>(g, w, bx))
 EGG_WRAP0(outer_ranges, 256, outer_ranges_body(g, w, bx, gx))
 EGG_WRAPD(cell_sums, 256, cell_sums_body<D>(g, w, bx))
@@ -557,31 +574,43 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_hist(Geom g, Work w, int
                                                              int shift) {
     radix_hist_body(g, w, in_sel, first, dim, shift, blockIdx.x);
 }
-__global__ void __launch_bounds__(kSortThreads) kb_radix_hist(BatchArgs B, int skip, int in_sel, int first, int dim,
-                                                              int shift) {
-    EGG_BATCH_ENTRY(B, skip);
-    (void)gx;
-    radix_hist_body(g, w, in_sel, first, dim, shift, bx);
-}
 __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(Geom g, Work w, int in_sel, int out_sel, int first,
                                                                 int dim, int shift) {
     radix_scatter_body(g, w, in_sel, out_sel, first, dim, shift, blockIdx.x);
 }
-__global__ void __launch_bounds__(kSortThreads) kb_radix_scatter(BatchArgs B, int skip, int in_sel, int out_sel,
-                                                                 int first, int dim, int shift) {
-    EGG_BATCH_ENTRY(B, skip);
-    (void)gx;
-    radix_scatter_body(g, w, in_sel, out_sel, first, dim, shift, bx);
+// batched radix passes: pass p of each instance's own plan
+__global__ void __launch_bounds__(kSortThreads) kb_radix_hist(BatchArgs B, int p) {
+    batch_for(B, [&](const Geom& g, const Work& w, int bx, int) {
+        const int count = plan_count(g);
+        if (p >= count) return;
+        int dim, shift;
+        plan_pass(g, p, dim, shift);
+        radix_hist_body(g, w, p > 0 ? plan_out_sel(count, p - 1) : 0, p == 0, dim, shift, bx);
+    });
+}
+__global__ void __launch_bounds__(256) kb_radix_scan(BatchArgs B, int p) {
+    batch_for(B, [&](const Geom& g, const Work& w, int bx, int) {
+        if (p >= plan_count(g)) return;
+        radix_scan_body(g, w, bx);
+    });
+}
+__global__ void __launch_bounds__(kSortThreads) kb_radix_scatter(BatchArgs B, int p) {
+    batch_for(B, [&](const Geom& g, const Work& w, int bx, int) {
+        const int count = plan_count(g);
+        if (p >= count) return;
+        int dim, shift;
+        plan_pass(g, p, dim, shift);
+        radix_scatter_body(g, w, p > 0 ? plan_out_sel(count, p - 1) : 0, plan_out_sel(count, p), p == 0, dim, shift,
+                           bx);
+    });
 }
 template <int D>
-__global__ void __launch_bounds__(kHeadsBlock) k_gather_heads(Geom g, Work w, int identity) {
-    gather_heads_body<D>(g, w, identity, blockIdx.x);
+__global__ void __launch_bounds__(kHeadsBlock) k_gather_heads(Geom g, Work w) {
+    gather_heads_body<D>(g, w, 0, blockIdx.x);
 }
 template <int D>
-__global__ void __launch_bounds__(kHeadsBlock) kb_gather_heads(BatchArgs B, int skip, int identity) {
-    EGG_BATCH_ENTRY(B, skip);
-    (void)gx;
-    gather_heads_body<D>(g, w, identity, bx);
+__global__ void __launch_bounds__(kHeadsBlock) kb_gather_heads(BatchArgs B) {
+    batch_for(B, [&](const Geom& g, const Work& w, int bx, int) { gather_heads_body<D>(g, w, 0, bx); });
 }
 
 // ---------------------------------------------------------------------------
@@ -644,37 +673,45 @@ __global__ void k_unsort_int(Geom g, Work w, const int* __restrict__ src, int* _
 #define EGG_GO(ex, shape, threads, st, NAME, ...)                                                     \
     do {                                                                                             \
         if ((ex).batch())                                                                            \
-            kb_##NAME<<<(ex).blocks(shape), threads, 0, st>>>((ex).args(shape), (ex).skip_done, ##__VA_ARGS__); \
+            kb_##NAME<<<(ex).blocks(shape, threads), threads, 0, st>>>((ex).args(shape), ##__VA_ARGS__); \
         else                                                                                         \
-            k_##NAME<<<(ex).blocks(shape), threads, 0, st>>>(*(ex).g, *(ex).w, ##__VA_ARGS__);       \
+            k_##NAME<<<(ex).blocks(shape, threads), threads, 0, st>>>(*(ex).g, *(ex).w, ##__VA_ARGS__); \
     } while (0)
 
 #define EGG_GO_D(ex, shape, threads, st, NAME, ...)                                                   \
     do {                                                                                             \
         if ((ex).batch()) {                                                                          \
             EGG_DISPATCH_D((ex).d, kb_##NAME,                                                        \
-                           <<<(ex).blocks(shape), threads, 0, st>>>((ex).args(shape), (ex).skip_done, ##__VA_ARGS__)); \
+                           <<<(ex).blocks(shape, threads), threads, 0, st>>>((ex).args(shape), ##__VA_ARGS__)); \
         } else {                                                                                     \
-            EGG_DISPATCH_D((ex).d, k_##NAME, <<<(ex).blocks(shape), threads, 0, st>>>(*(ex).g, *(ex).w, ##__VA_ARGS__)); \
+            EGG_DISPATCH_D((ex).d, k_##NAME,                                                         \
+                           <<<(ex).blocks(shape, threads), threads, 0, st>>>(*(ex).g, *(ex).w, ##__VA_ARGS__)); \
         }                                                                                            \
     } while (0)
 
-void launch_build(const Exec& ex, const SortPlan& plan, cudaStream_t st) {
+void launch_build(const Exec& ex, cudaStream_t st) {
     EGG_GO(ex, kShapeOne, 32, st, build_begin);
     EGG_GO_D(ex, kShapeCapN256, 256, st, check_cells);
-    // radix passes; the last one must land in perm (selector 0)
-    int out = (plan.count % 2 == 1) ? 0 : 1;
-    int in = 0;
-    for (int p = 0; p < plan.count; p++) {
-        const int first = (p == 0);
-        EGG_GO(ex, kShapeTiles, kSortThreads, st, radix_hist, in, first, plan.dim[p], plan.shift[p]);
-        EGG_GO(ex, kShapeDigits, 256, st, radix_scan);
-        EGG_GO(ex, kShapeTiles, kSortThreads, st, radix_scatter, in, out, first, plan.dim[p], plan.shift[p]);
-        in = out;
-        out ^= 1;
+    if (ex.batch()) {
+        for (int p = 0; p < ex.bt->max_passes; p++) {
+            kb_radix_hist<<<ex.blocks(kShapeTiles, kSortThreads), kSortThreads, 0, st>>>(ex.args(kShapeTiles), p);
+            kb_radix_scan<<<ex.blocks(kShapeDigits, 256), 256, 0, st>>>(ex.args(kShapeDigits), p);
+            kb_radix_scatter<<<ex.blocks(kShapeTiles, kSortThreads), kSortThreads, 0, st>>>(ex.args(kShapeTiles), p);
+        }
+    } else {
+        const Geom& g = *ex.g;
+        const int count = plan_count(g);
+        for (int p = 0; p < count; p++) {
+            int dim, shift;
+            plan_pass(g, p, dim, shift);
+            const int in = p > 0 ? plan_out_sel(count, p - 1) : 0, out = plan_out_sel(count, p);
+            const int tiles = shape_blocks(kShapeTiles, g);
+            k_radix_hist<<<tiles, kSortThreads, 0, st>>>(g, *ex.w, in, p == 0, dim, shift);
+            k_radix_scan<<<shape_blocks(kShapeDigits, g), 256, 0, st>>>(g, *ex.w);
+            k_radix_scatter<<<tiles, kSortThreads, 0, st>>>(g, *ex.w, in, out, p == 0, dim, shift);
+        }
     }
-    const int identity = plan.count == 0;
-    EGG_GO_D(ex, kShapeN1024, kHeadsBlock, st, gather_heads, identity);
+    EGG_GO_D(ex, kShapeN1024, kHeadsBlock, st, gather_heads);
     EGG_GO(ex, kShapeOne, 1024, st, scan_block_sums);
     EGG_GO_D(ex, kShapeN1024, kHeadsBlock, st, heads_finalize);
     EGG_GO(ex, kShapeOuter, 256, st, outer_ranges);

@@ -26,31 +26,17 @@
 
 #include "eggsync.h"
 #include "egg_common.cuh"
+#include "egg_host_common.h"
 #include "egg_kernels.h"
 
 namespace egg {
 
-namespace {
-
-thread_local std::string g_last_error;
 std::mutex g_mutex;
+thread_local std::string g_last_error;
+// interaction counters of the last run (stats build)
+unsigned long long g_counters[kUStats] = {};
 
-struct CudaError {
-    cudaError_t code;
-    std::string where;
-};
-
-#define EGG_CHECK(call)                                                              \
-    do {                                                                             \
-        cudaError_t _e = (call);                                                     \
-        if (_e != cudaSuccess) throw CudaError{_e, std::string(#call) + " @" +       \
-                                                     std::to_string(__LINE__)};      \
-    } while (0)
-
-struct ArgError {
-    int status;
-    std::string msg;
-};
+namespace {
 
 // ------------------------------------------------------------------------
 // geometry, stencils, tables
@@ -64,6 +50,8 @@ float sq_threshold(float e) {
     }
     return t;
 }
+
+}  // namespace
 
 // EGG_SynC.cu:1249-1260, 1430, 563, 779, 1045
 Geom make_geom(int64_t n64, int d, float eps) {
@@ -107,33 +95,6 @@ Geom make_geom(int64_t n64, int d, float eps) {
     return g;
 }
 
-SortPlan make_plan(const Geom& g) {
-    SortPlan P;
-    auto add_dim = [&](int l) {
-        P.dim[P.count] = l;
-        P.shift[P.count] = 0;
-        P.count++;
-        if (g.width > 256) {
-            P.dim[P.count] = l;
-            P.shift[P.count] = 8;
-            P.count++;
-        }
-    };
-    // least significant first: the sub-cell key (order inside a cell), then
-    // g_{d-1}, ..., g_od, then g_0, ..., g_{od-1}
-    P.dim[P.count] = -1;
-    P.shift[P.count] = 0;
-    P.count++;
-    for (int l = g.d - 1; l >= g.od; l--) add_dim(l);
-    for (int l = 0; l < g.od; l++) add_dim(l);
-    return P;
-}
-
-struct Stencil {
-    std::vector<int> delta;
-    std::vector<signed char> off;
-};
-
 Stencil make_stencil(const Geom& g, int rad) {
     Stencil S;
     const int od = g.od;
@@ -163,7 +124,103 @@ Stencil make_stencil(const Geom& g, int rad) {
     return S;
 }
 
-size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
+bool is_device_ptr(const void* p) {
+    cudaPointerAttributes a;
+    cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+size_t layout_work(const Geom& g, int max_iter, char* base, Work& w, float** xin, bool own_io) {
+    const int d = g.d;
+    const size_t ns = (size_t)g.ns;
+    const int tiles = (g.n + kSortTile - 1) / kSortTile;
+    const int nb = (g.n + kHeadsBlock - 1) / kHeadsBlock;
+    const int nw = (g.n + 31) / 32;
+    size_t off = 0;
+    auto add = [&](void** p, size_t bytes) {
+        *p = base ? base + off : nullptr;
+        off += align_up(bytes);
+    };
+    add((void**)&w.X, 4 * d * ns);
+    add((void**)&w.Xn, 4 * d * ns);
+    add((void**)&w.sd, 4 * d * ns);
+    add((void**)&w.md, 4 * d * ns);
+    add((void**)&w.qlo, 4 * d * ns);
+    add((void**)&w.qhi, 4 * d * ns);
+    add((void**)&w.ulo, 4 * d * ns);
+    add((void**)&w.uhi, 4 * d * ns);
+    add((void**)&w.orig, 4 * ns);
+    add((void**)&w.orig_tmp, 4 * ns);
+    add((void**)&w.perm, 4 * ns);
+    add((void**)&w.perm_tmp, 4 * ns);
+    add((void**)&w.cell_of, 4 * ns);
+    add((void**)&w.cell_start, 4 * (ns + 1));
+    add((void**)&w.cell_dims, 4 * d * ns);
+    add((void**)&w.cell_outer, 4 * ns);
+    add((void**)&w.css, 4 * d * ns);
+    add((void**)&w.csm, 4 * d * ns);
+    add((void**)&w.cbmin, 4 * d * ns);
+    add((void**)&w.cbmax, 4 * d * ns);
+    add((void**)&w.outer_begin, 4 * ((size_t)g.n_outer + 1));
+    add((void**)&w.hist, 4 * 256 * (size_t)tiles);
+    add((void**)&w.digit_total, 4 * 256);
+    add((void**)&w.block_sums, 4 * (size_t)nb);
+    add((void**)&w.wpart, 8 * 4 * (size_t)d * 2 * nw);
+    add((void**)&w.gpart, 4 * 4 * (size_t)d * 2 * nw);
+    add((void**)&w.ctrl, 4 * kCtrlWords);
+    add((void**)&w.ustats, 8 * kUStats);
+    add((void**)&w.stamps, 8 * 4 * ((size_t)max_iter + 2));
+    add((void**)&w.iter_flags, 4 * ((size_t)max_iter + 2));
+    add((void**)&w.dirty[0], (size_t)g.n_outer + 1);
+    add((void**)&w.dirty[1], (size_t)g.n_outer + 1);
+    add((void**)&w.need, (size_t)g.n_outer + 1);
+    add((void**)&w.viol_orig, ns);
+    add((void**)&w.span_list, 4 * ((size_t)nw + 1));
+    add((void**)&w.big_list, 4 * ((size_t)nw / 4 + 1));
+    add((void**)&w.rpart, 8 * 2 * (size_t)((g.n + 127) / 128));
+    add((void**)&w.rvals, 8 * 2 * ((size_t)max_iter + 2));
+    add((void**)&w.uf_parent, 4 * ns);
+    add((void**)&w.uf_size, 4 * ns);
+    if (own_io) {
+        const Consts c = make_consts(g);
+        add((void**)&w.st_delta, 4 * c.st_delta.size());
+        add((void**)&w.st_off, c.st_off.size());
+        add((void**)&w.table, 4 * c.table.size());
+        add((void**)&w.labels, 4 * ns);
+        add((void**)xin, 4 * (size_t)g.n * d);
+    }
+    return off;
+}
+
+Consts make_consts(const Geom& g) {
+    Consts c;
+    Stencil st[3] = {make_stencil(g, g.r), make_stencil(g, g.r_extra), make_stencil(g, g.r_half)};
+    for (auto& s : st) c.st_cap = std::max(c.st_cap, (int)s.delta.size());
+    const int odp = std::max(g.od, 1);
+    const int TW = 2 * g.table_k + 1;
+    c.st_delta.assign(3 * (size_t)c.st_cap, 0);
+    c.st_off.assign(3 * (size_t)c.st_cap * odp, 0);
+    for (int k = 0; k < 3; k++) {
+        c.st_count[k] = (int)st[k].delta.size();
+        std::copy(st[k].delta.begin(), st[k].delta.end(), c.st_delta.begin() + (size_t)k * c.st_cap);
+        std::copy(st[k].off.begin(), st[k].off.end(), c.st_off.begin() + (size_t)k * c.st_cap * odp);
+    }
+    c.table.resize(3 * (size_t)TW);
+    for (int k = -g.table_k; k <= g.table_k; k++) {
+        const double a = (double)k * (double)g.side;
+        const double sh = sin(0.5 * a);
+        c.table[k + g.table_k] = (float)sin(a);
+        c.table[TW + k + g.table_k] = (float)cos(a);
+        c.table[2 * TW + k + g.table_k] = (float)(2.0 * sh * sh);
+    }
+    return c;
+}
+
+namespace {
 
 // ------------------------------------------------------------------------
 // per-device instance: workspace, stream, graph
@@ -181,7 +238,6 @@ struct Instance {
     // current layout
     Geom g;
     Work w;
-    SortPlan plan;
     float* xin = nullptr;                  // staging for host input (n*d)
     int max_iter = 0;
     size_t used = 0;
@@ -217,68 +273,10 @@ Instance& instance() {
 // Lay out the workspace for geometry g (allocating or growing it) and
 // upload the stencils and tables.
 void prepare(Instance& I, const Geom& g, int max_iter) {
-    const int d = g.d;
-    const size_t ns = (size_t)g.ns;
-    const int tiles = (g.n + kSortTile - 1) / kSortTile;
-    const int nb = (g.n + kHeadsBlock - 1) / kHeadsBlock;
-    const int nw = (g.n + 31) / 32;
-    Stencil st[3] = {make_stencil(g, g.r), make_stencil(g, g.r_extra), make_stencil(g, g.r_half)};
-    int st_cap = 1;
-    for (auto& s : st) st_cap = std::max(st_cap, (int)s.delta.size());
-    const int odp = std::max(g.od, 1);
-    const int TW = 2 * g.table_k + 1;
-
-    size_t off = 0;
-    std::vector<std::pair<void**, size_t>> plan;
     Work w;
     memset(&w, 0, sizeof(w));
     float* xin = nullptr;
-    auto add = [&](void** p, size_t bytes) { plan.push_back({p, bytes}); };
-    add((void**)&w.X, 4 * d * ns);
-    add((void**)&w.Xn, 4 * d * ns);
-    add((void**)&w.sd, 4 * d * ns);
-    add((void**)&w.md, 4 * d * ns);
-    add((void**)&w.qlo, 4 * d * ns);
-    add((void**)&w.qhi, 4 * d * ns);
-    add((void**)&w.ulo, 4 * d * ns);
-    add((void**)&w.uhi, 4 * d * ns);
-    add((void**)&w.orig, 4 * ns);
-    add((void**)&w.orig_tmp, 4 * ns);
-    add((void**)&w.perm, 4 * ns);
-    add((void**)&w.perm_tmp, 4 * ns);
-    add((void**)&w.cell_of, 4 * ns);
-    add((void**)&w.cell_start, 4 * (ns + 1));
-    add((void**)&w.cell_dims, 4 * d * ns);
-    add((void**)&w.cell_outer, 4 * ns);
-    add((void**)&w.css, 4 * d * ns);
-    add((void**)&w.csm, 4 * d * ns);
-    add((void**)&w.cbmin, 4 * d * ns);
-    add((void**)&w.cbmax, 4 * d * ns);
-    add((void**)&w.outer_begin, 4 * ((size_t)g.n_outer + 1));
-    add((void**)&w.hist, 4 * 256 * (size_t)tiles);
-    add((void**)&w.digit_total, 4 * 256);
-    add((void**)&w.block_sums, 4 * (size_t)nb);
-    add((void**)&w.wpart, 8 * 4 * (size_t)d * 2 * nw);
-    add((void**)&w.gpart, 4 * 4 * (size_t)d * 2 * nw);
-    add((void**)&w.st_delta, 4 * 3 * (size_t)st_cap);
-    add((void**)&w.st_off, 3 * (size_t)st_cap * odp);
-    add((void**)&w.table, 4 * 3 * (size_t)TW);
-    add((void**)&w.ctrl, 4 * kCtrlWords);
-    add((void**)&w.stamps, 8 * 4 * ((size_t)max_iter + 2));
-    add((void**)&w.labels, 4 * ns);
-    add((void**)&w.iter_flags, 4 * ((size_t)max_iter + 2));
-    add((void**)&xin, 4 * (size_t)g.n * d);
-    add((void**)&w.dirty[0], (size_t)g.n_outer + 1);
-    add((void**)&w.dirty[1], (size_t)g.n_outer + 1);
-    add((void**)&w.need, (size_t)g.n_outer + 1);
-    add((void**)&w.viol_orig, ns);
-    add((void**)&w.span_list, 4 * ((size_t)nw + 1));
-    add((void**)&w.big_list, 4 * ((size_t)nw / 4 + 1));
-    add((void**)&w.rpart, 8 * 2 * (size_t)((g.n + 127) / 128));
-    add((void**)&w.rvals, 8 * 2 * ((size_t)max_iter + 2));
-    add((void**)&w.uf_parent, 4 * ns);
-    add((void**)&w.uf_size, 4 * ns);
-    for (auto& p : plan) off += align_up(p.second);
+    const size_t off = layout_work(g, max_iter, nullptr, w, &xin, true);
     if (off > I.cap) {
         destroy_graph(I);
         if (I.base) EGG_CHECK(cudaFree(I.base));
@@ -288,33 +286,15 @@ void prepare(Instance& I, const Geom& g, int max_iter) {
         EGG_CHECK(cudaMalloc(&I.base, want));
         I.cap = want;
     }
-    char* b = (char*)I.base;
-    for (auto& p : plan) {
-        *p.first = b;
-        b += align_up(p.second);
-    }
+    layout_work(g, max_iter, (char*)I.base, w, &xin, true);
     I.used = off;
-    w.st_cap = st_cap;
-    for (int k = 0; k < 3; k++) w.st_count[k] = (int)st[k].delta.size();
-
-    // stencils and tables (pageable copies are synchronous; sizes are small)
-    std::vector<int> hd(3 * (size_t)st_cap, 0);
-    std::vector<signed char> ho(3 * (size_t)st_cap * odp, 0);
-    for (int k = 0; k < 3; k++) {
-        std::copy(st[k].delta.begin(), st[k].delta.end(), hd.begin() + (size_t)k * st_cap);
-        std::copy(st[k].off.begin(), st[k].off.end(), ho.begin() + (size_t)k * st_cap * odp);
-    }
-    std::vector<float> tab(3 * (size_t)TW);
-    for (int k = -g.table_k; k <= g.table_k; k++) {
-        const double a = (double)k * (double)g.side;
-        const double sh = sin(0.5 * a);
-        tab[k + g.table_k] = (float)sin(a);
-        tab[TW + k + g.table_k] = (float)cos(a);
-        tab[2 * TW + k + g.table_k] = (float)(2.0 * sh * sh);
-    }
-    EGG_CHECK(cudaMemcpyAsync(w.st_delta, hd.data(), hd.size() * 4, cudaMemcpyHostToDevice, I.st));
-    EGG_CHECK(cudaMemcpyAsync(w.st_off, ho.data(), ho.size(), cudaMemcpyHostToDevice, I.st));
-    EGG_CHECK(cudaMemcpyAsync(w.table, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice, I.st));
+    const Consts c = make_consts(g);
+    w.st_cap = c.st_cap;
+    for (int k = 0; k < 3; k++) w.st_count[k] = c.st_count[k];
+    // pageable copies are synchronous; sizes are small
+    EGG_CHECK(cudaMemcpyAsync(w.st_delta, c.st_delta.data(), c.st_delta.size() * 4, cudaMemcpyHostToDevice, I.st));
+    EGG_CHECK(cudaMemcpyAsync(w.st_off, c.st_off.data(), c.st_off.size(), cudaMemcpyHostToDevice, I.st));
+    EGG_CHECK(cudaMemcpyAsync(w.table, c.table.data(), c.table.size() * 4, cudaMemcpyHostToDevice, I.st));
     EGG_CHECK(cudaStreamSynchronize(I.st));
 
     if ((int)((max_iter + 2) * 4) > I.h_stamps_cap) {
@@ -324,7 +304,6 @@ void prepare(Instance& I, const Geom& g, int max_iter) {
     }
     I.g = g;
     I.w = w;
-    I.plan = make_plan(g);
     I.xin = xin;
     I.max_iter = max_iter;
 }
@@ -334,6 +313,7 @@ void prepare(Instance& I, const Geom& g, int max_iter) {
 // ------------------------------------------------------------------------
 __global__ void k_ctrl_reset(Work w, int max_iter, int full_update) {
     for (int t = threadIdx.x; t < kCtrlWords; t += blockDim.x) w.ctrl[t] = 0;
+    for (int t = threadIdx.x; t < kUStats; t += blockDim.x) w.ustats[t] = 0;
     __syncwarp();
     if (threadIdx.x == 0) {
         w.ctrl[kCtrlMaxIter] = max_iter;
@@ -379,7 +359,7 @@ void enqueue_iteration(Instance& I, cudaGraphConditionalHandle h, int in_graph, 
     };
     k_iter_begin<<<1, 1, 0, st>>>(I.w);
     mark(0);
-    launch_build(single(I.g, I.w), I.plan, st);
+    launch_build(single(I.g, I.w), st);
     mark(1);
     mark(2);
     launch_cell_sums(single(I.g, I.w), st);
@@ -440,16 +420,6 @@ bool ensure_graph(Instance& I) {
     return true;
 }
 
-bool is_device_ptr(const void* p) {
-    cudaPointerAttributes a;
-    cudaError_t e = cudaPointerGetAttributes(&a, p);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
-
 // load x (host or device, row-major n x d) into Xn and reset the control words
 void load_input(Instance& I, const float* x, int full_update = 0) {
     const Geom& g = I.g;
@@ -475,29 +445,6 @@ void order_after(Instance& I, void* stream) {
     cudaStream_t cs = (cudaStream_t)stream;
     EGG_CHECK(cudaEventRecord(I.ev[5], cs));
     EGG_CHECK(cudaStreamWaitEvent(I.st, I.ev[5], 0));
-}
-
-int fail(int status, const std::string& msg) {
-    g_last_error = msg;
-    return status;
-}
-
-template <typename F>
-int guarded(F&& fn) {
-    std::lock_guard<std::mutex> lock(g_mutex);
-    g_last_error.clear();
-    try {
-        return fn();
-    } catch (const ArgError& e) {
-        return fail(e.status, e.msg);
-    } catch (const CudaError& e) {
-        cudaGetLastError();
-        return fail(e.code == cudaErrorNoDevice || e.code == cudaErrorInsufficientDriver ? EGG_ERR_NO_DEVICE
-                                                                                          : EGG_ERR_CUDA,
-                    std::string(cudaGetErrorString(e.code)) + " in " + e.where);
-    } catch (const std::bad_alloc&) {
-        return fail(EGG_ERR_INTERNAL, "host allocation failed");
-    }
 }
 
 }  // namespace
@@ -554,7 +501,7 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
     }
     EGG_CHECK(cudaEventRecord(I.ev[2], I.st));
     // final grid and labels (EGG_SynC.cu:1503-1522)
-    launch_build(single(I.g, I.w), I.plan, I.st);
+    launch_build(single(I.g, I.w), I.st);
     const bool dev_out = is_device_ptr(labels);
     int* lab = dev_out ? labels : I.w.labels;
     if (opts.labels_mode == 1) launch_labels(I.g, I.w, lab, I.st);
@@ -581,6 +528,9 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
 
     const int iters = I.h_ctrl[kCtrlIter];
     const int converged = (g.stop_rule ? I.h_ctrl[kCtrlLamReached] : I.h_ctrl[kCtrlFlag]) != 0;
+#ifdef EGG_UPDATE_STATS
+    EGG_CHECK(cudaMemcpy(g_counters, I.w.ustats, sizeof(g_counters), cudaMemcpyDeviceToHost));
+#endif
     if (stats) {
         const int M = I.h_ctrl[kCtrlM];
         stats->iterations = iters;
@@ -636,7 +586,7 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
         // [2 order parameter], update, mark, 3 extra check, end; then the
         // final build, labels (1 or 4 kernels), [2 cell sums + 2 order
         // parameter], [positions]
-        const int build_l = 3 * I.plan.count + 6;
+        const int build_l = 3 * plan_count(g) + 6;
         const int per_iter = build_l + 10 + ((g.order_mode == 2 || g.stop_rule == 1) ? 2 : 0);
         const int final_l = build_l + (opts.labels_mode == 1 ? 1 : 4) + (g.order_mode == 1 ? 4 : 0) +
                             (opts.positions_out ? 1 : 0);
@@ -659,7 +609,7 @@ int step(const float* x, int64_t n, int32_t d, float eps, float* x_next, int32_t
     check_status_bits(I);
     cudaStream_t st = I.st;
     k_iter_begin<<<1, 1, 0, st>>>(I.w);
-    launch_build(single(I.g, I.w), I.plan, st);
+    launch_build(single(I.g, I.w), st);
     launch_cell_sums(single(I.g, I.w), st);
     launch_need(single(I.g, I.w), st);
     int* cnt_sorted = I.w.orig_tmp;  // free once the grid is built
@@ -697,7 +647,7 @@ int grid(const float* x, int64_t n, int32_t d, float eps, int32_t* order, int32_
     prepare(I, g, 4);
     load_input(I, x);
     check_status_bits(I);
-    launch_build(single(I.g, I.w), I.plan, I.st);
+    launch_build(single(I.g, I.w), I.st);
     EGG_CHECK(cudaMemcpyAsync(I.h_ctrl, I.w.ctrl, kCtrlWords * sizeof(int), cudaMemcpyDeviceToHost, I.st));
     EGG_CHECK(cudaStreamSynchronize(I.st));
     const int M = I.h_ctrl[kCtrlM];
@@ -794,7 +744,6 @@ int grid_noalloc(const float* x, int64_t n, int32_t d, float eps, int32_t* order
     if (off > kNoAllocBytes) throw ArgError{EGG_ERR_INTERNAL, "static scratch too small for this geometry"};
 
     cudaStream_t st = (cudaStream_t)stream;
-    const SortPlan plan = make_plan(g);
     // the array keeps the previous call's contents: the control words must
     // start at zero (every other buffer is fully written before it is read)
     k_noalloc_reset<<<1, 32, 0, st>>>(w.ctrl);
@@ -804,7 +753,7 @@ int grid_noalloc(const float* x, int64_t n, int32_t d, float eps, int32_t* order
         src = xin;
     }
     launch_transpose_in(g, w, src, st);
-    launch_build(single(g, w), plan, st);
+    launch_build(single(g, w), st);
     int ctrl_h[kCtrlWords];
     EGG_CHECK(cudaMemcpyAsync(ctrl_h, w.ctrl, sizeof(ctrl_h), cudaMemcpyDeviceToHost, st));
     EGG_CHECK(cudaStreamSynchronize(st));
@@ -820,6 +769,7 @@ int grid_noalloc(const float* x, int64_t n, int32_t d, float eps, int32_t* order
 }
 
 int release() {
+    release_batch();
     for (auto& kv : g_inst) {
         Instance* I = kv.second;
         int cur = 0;
@@ -899,5 +849,17 @@ __attribute__((visibility("default"))) int egg_release(void) {
 }
 
 __attribute__((visibility("default"))) int egg_abi_version(void) { return EGG_SYNC_ABI_VERSION; }
+
+__attribute__((visibility("default"))) int egg_update_counters(int64_t* out, int32_t cap) {
+#ifdef EGG_UPDATE_STATS
+    std::lock_guard<std::mutex> lock(egg::g_mutex);
+    for (int k = 0; k < egg::kUStats && k < cap; k++) out[k] = (int64_t)egg::g_counters[k];
+    return egg::kUStats;
+#else
+    (void)out;
+    (void)cap;
+    return 0;
+#endif
+}
 
 }  // extern "C"

@@ -13,36 +13,42 @@
 
 namespace egg {
 
-// LSD radix passes over the cell digits: pass p sorts on
-// (cell_dim(x[dim[p]]) >> shift[p]) & 255, least significant pass first;
-// dim[p] < 0 is the within-cell sub-cell key.
-struct SortPlan {
-    int count = 0;
-    int dim[2 * kMaxDims + 1];
-    int shift[2 * kMaxDims + 1];
-};
-
+// A batch of instances: device descriptors plus one active list with its
+// per-shape virtual-block offsets (egg_batch.cuh).
 struct BatchTables {
-    const Geom* geoms = nullptr;  // device [ninst]
-    const Work* works = nullptr;  // device [ninst]
-    const int* boff = nullptr;    // device [kShapeCount][ninst + 1]
-    int total[kShapeCount] = {};  // blocks per shape over the batch
-    int ninst = 0;
+    const Geom* geoms = nullptr;  // device [instances]
+    const Work* works = nullptr;  // device [instances]
+    const int* boff = nullptr;    // device [kShapeCount][cap + 1]
+    const int* active = nullptr;  // device [cap]
+    const int* nact = nullptr;    // device [1]
+    int cap = 0;                  // list capacity
+    int total[kShapeCount] = {};  // virtual blocks per shape over all instances
+    int max_passes = 0;           // radix passes of the instance with the most
     int max_table_k = 0;
+    int occ = 8;                  // persistent blocks per SM of a 256-thread kernel
+    int update_threads = 128;     // block size of the update kernel: 64, 128 or 256
 };
 
 struct Exec {
     const Geom* g = nullptr;           // single instance (host objects)
     const Work* w = nullptr;
     const BatchTables* bt = nullptr;   // batch
-    int skip_done = 1;                 // batch: blocks of finished instances return at once
     int d = 0;                         // dimensions (kernel template)
     bool batch() const { return bt != nullptr; }
-    int blocks(int shape) const { return bt ? bt->total[shape] : shape_blocks(shape, *g); }
+    // single: the shape's block count; batch: a persistent grid
+    int blocks(int shape, int threads) const {
+        if (!bt) return shape_blocks(shape, *g);
+        int per_sm = bt->occ * 256 / threads;
+        if (per_sm < 1) per_sm = 1;
+        const int cap = 148 * per_sm;
+        const int t = bt->total[shape];
+        return t < 1 ? 1 : (t < cap ? t : cap);
+    }
     BatchArgs args(int shape) const {
-        return BatchArgs{bt->geoms, bt->works, bt->boff + (size_t)shape * (bt->ninst + 1), bt->ninst};
+        return BatchArgs{bt->geoms, bt->works, bt->boff + (size_t)shape * (bt->cap + 1), bt->active, bt->nact};
     }
     int table_k() const { return bt ? bt->max_table_k : g->table_k; }
+    int update_threads() const { return bt ? bt->update_threads : 128; }
 };
 
 inline Exec single(const Geom& g, const Work& w) {
@@ -53,15 +59,25 @@ inline Exec single(const Geom& g, const Work& w) {
     return e;
 }
 
+inline Exec batched(const BatchTables& bt, int d) {
+    Exec e;
+    e.bt = &bt;
+    e.d = d;
+    return e;
+}
+
 // grid (egg_grid.cu)
-void launch_build(const Exec& ex, const SortPlan& plan, cudaStream_t st);
+// the grid of the current positions Xn (radix passes: plan_count/plan_pass)
+void launch_build(const Exec& ex, cudaStream_t st);
 void launch_cell_sums(const Exec& ex, cudaStream_t st);
 void launch_transpose_in(const Geom& g, const Work& w, const float* x, cudaStream_t st);
 void launch_unsort_positions(const Geom& g, const Work& w, const float* src, float* out, cudaStream_t st);
 void launch_labels(const Geom& g, const Work& w, int* out, cudaStream_t st);
 void launch_unsort_int(const Geom& g, const Work& w, const int* src, int* out, cudaStream_t st);
-// union-find labelling (egg_labels.cu): same partition and values as launch_labels
+// union-find labelling (egg_labels.cu): same partition and values as
+// launch_labels; a batch writes each instance's labels to its w.labels
 void launch_labels_uf(const Geom& g, const Work& w, int* out, cudaStream_t st);
+void launch_labels_uf(const Exec& ex, cudaStream_t st);
 
 // update + flag (egg_update.cu); counts (nullable, single instance only)
 // receives |N_eps(p)| per sorted point

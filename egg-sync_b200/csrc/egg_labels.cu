@@ -45,46 +45,72 @@ __device__ __forceinline__ void uf_union(int* parent, int a, int b) {
 
 }  // namespace
 
-__global__ void k_uf_init(Geom g, int* __restrict__ parent, int* __restrict__ csize) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
-        parent[i] = i;
-        csize[i] = 0;
+__device__ __forceinline__ void uf_init_body(const Geom& g, const Work& w, int bx, int gx) {
+    for (int i = bx * blockDim.x + threadIdx.x; i < g.n; i += gx * blockDim.x) {
+        w.uf_parent[i] = i;
+        w.uf_size[i] = 0;
     }
 }
 
 // edge (i, i+1) whenever both points lie in the same final cell
-__global__ void k_uf_link(Geom g, Work w, int* parent) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i + 1 < g.n; i += gridDim.x * blockDim.x)
-        if (w.cell_of[i] == w.cell_of[i + 1]) uf_union(parent, i, i + 1);
+__device__ __forceinline__ void uf_link_body(const Geom& g, const Work& w, int bx, int gx) {
+    for (int i = bx * blockDim.x + threadIdx.x; i + 1 < g.n; i += gx * blockDim.x)
+        if (w.cell_of[i] == w.cell_of[i + 1]) uf_union(w.uf_parent, i, i + 1);
 }
 
-__global__ void k_uf_compress(Geom g, int* parent, int* csize) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
-        const int r = uf_find(parent, i);
-        atomicAdd(csize + r, 1);
+__device__ __forceinline__ void uf_compress_body(const Geom& g, const Work& w, int bx, int gx) {
+    for (int i = bx * blockDim.x + threadIdx.x; i < g.n; i += gx * blockDim.x) {
+        const int r = uf_find(w.uf_parent, i);
+        atomicAdd(w.uf_size + r, 1);
     }
 }
 
-__global__ void k_uf_labels(Geom g, Work w, const int* __restrict__ parent, const int* __restrict__ csize,
-                            int* __restrict__ out) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+__device__ __forceinline__ void uf_labels_body(const Geom& g, const Work& w, int* __restrict__ out, int bx, int gx) {
+    const int* parent = w.uf_parent;
+    for (int i = bx * blockDim.x + threadIdx.x; i < g.n; i += gx * blockDim.x) {
         // parent[i] may still point to a non-root after compress (halving),
         // so follow it to the root without writing
         int r = parent[i];
         while (parent[r] != r) r = parent[r];
-        const bool multi = csize[r] > 1;
+        const bool multi = w.uf_size[r] > 1;
         out[w.orig[i]] = multi ? w.cell_of[r] : -1;
         if (multi && r == i) atomicAdd(w.ctrl + kCtrlClusters, 1);
     }
 }
 
+__global__ void k_uf_init(Geom g, Work w) { uf_init_body(g, w, blockIdx.x, gridDim.x); }
+__global__ void k_uf_link(Geom g, Work w) { uf_link_body(g, w, blockIdx.x, gridDim.x); }
+__global__ void k_uf_compress(Geom g, Work w) { uf_compress_body(g, w, blockIdx.x, gridDim.x); }
+__global__ void k_uf_labels(Geom g, Work w, int* out) { uf_labels_body(g, w, out, blockIdx.x, gridDim.x); }
+
+__global__ void kb_uf_init(BatchArgs B) {
+    batch_for(B, [&](const Geom& g, const Work& w, int bx, int gx) { uf_init_body(g, w, bx, gx); });
+}
+__global__ void kb_uf_link(BatchArgs B) {
+    batch_for(B, [&](const Geom& g, const Work& w, int bx, int gx) { uf_link_body(g, w, bx, gx); });
+}
+__global__ void kb_uf_compress(BatchArgs B) {
+    batch_for(B, [&](const Geom& g, const Work& w, int bx, int gx) { uf_compress_body(g, w, bx, gx); });
+}
+__global__ void kb_uf_labels(BatchArgs B) {
+    batch_for(B, [&](const Geom& g, const Work& w, int bx, int gx) { uf_labels_body(g, w, w.labels, bx, gx); });
+}
+
 void launch_labels_uf(const Geom& g, const Work& w, int* out, cudaStream_t st) {
-    int blocks = (g.n + 255) / 256;
-    if (blocks > 148 * 16) blocks = 148 * 16;
-    k_uf_init<<<blocks, 256, 0, st>>>(g, w.uf_parent, w.uf_size);
-    k_uf_link<<<blocks, 256, 0, st>>>(g, w, w.uf_parent);
-    k_uf_compress<<<blocks, 256, 0, st>>>(g, w.uf_parent, w.uf_size);
-    k_uf_labels<<<blocks, 256, 0, st>>>(g, w, w.uf_parent, w.uf_size, out);
+    const int blocks = shape_blocks(kShapeCapN256L, g);
+    k_uf_init<<<blocks, 256, 0, st>>>(g, w);
+    k_uf_link<<<blocks, 256, 0, st>>>(g, w);
+    k_uf_compress<<<blocks, 256, 0, st>>>(g, w);
+    k_uf_labels<<<blocks, 256, 0, st>>>(g, w, out);
+}
+
+void launch_labels_uf(const Exec& ex, cudaStream_t st) {
+    const int blocks = ex.blocks(kShapeCapN256L, 256);
+    const BatchArgs B = ex.args(kShapeCapN256L);
+    kb_uf_init<<<blocks, 256, 0, st>>>(B);
+    kb_uf_link<<<blocks, 256, 0, st>>>(B);
+    kb_uf_compress<<<blocks, 256, 0, st>>>(B);
+    kb_uf_labels<<<blocks, 256, 0, st>>>(B);
 }
 
 }  // namespace egg

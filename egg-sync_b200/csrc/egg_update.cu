@@ -79,6 +79,12 @@ __device__ int half_count(const Geom& g, const Work& w, const float* x, const in
 
 namespace {
 
+#ifdef EGG_UPDATE_STATS
+#define EGG_STAT(a, k, v) ((a).st[k] += (v))
+#else
+#define EGG_STAT(a, k, v) ((void)0)
+#endif
+
 template <int D>
 struct Acc {
     float S[D > 0 ? D : kMaxDims];
@@ -86,6 +92,9 @@ struct Acc {
     int N;
     int partial_in;
     bool tab_err;
+#ifdef EGG_UPDATE_STATS
+    unsigned st[kUStats];
+#endif
 };
 
 // m counted points of a cell at offsets k (= cell dims - own dims) with
@@ -117,15 +126,23 @@ __device__ __forceinline__ void visit_cell(const Geom& g, const Work& w, int c, 
         box_terms(x[l], cd, g.side, sm2, lg2);
         kk[l] = cd - gi[l];
     }
+    EGG_STAT(a, kUsCells, 1);
     if (!(sm2 <= g.t_eps)) return;
+    EGG_STAT(a, kUsSmallPass, 1);
     const int qb = __ldg(w.cell_start + c), qe = __ldg(w.cell_start + c + 1);
     bool all_in = lg2 <= g.t_eps;
     const bool full = all_in;
     if (!full) {
         float near2, far2;
         tight_box_dist2(x, w.cbmin + c, w.cbmax + c, g.ns, d, near2, far2);
-        if (near2 > g.t_eps) return;
+        if (near2 > g.t_eps) {
+            EGG_STAT(a, kUsTightOut, 1);
+            return;
+        }
         all_in = far2 <= g.t_eps;
+        if (all_in) EGG_STAT(a, kUsTightIn, 1);
+    } else {
+        EGG_STAT(a, kUsFull, 1);
     }
     if (all_in) {
         float SS[DM], SM[DM];
@@ -158,8 +175,12 @@ __device__ __forceinline__ void visit_cell(const Geom& g, const Work& w, int c, 
                 n2 = __fmaf_rn(a0, a0, n2);
                 f2 = __fmaf_rn(b0, b0, f2);
             }
-            if (n2 > g.t_eps) continue;
+            if (n2 > g.t_eps) {
+                EGG_STAT(a, kUsGroupsOut, 1);
+                continue;
+            }
             if (f2 <= g.t_eps) {
+                EGG_STAT(a, kUsGroupsIn, 1);
                 for (int l = 0; l < d; l++) {
                     as[l] += __ldg(w.gpart + wp_idx_f(0, l, d, rec, nw, k));
                     am[l] += __ldg(w.gpart + wp_idx_f(1, l, d, rec, nw, k));
@@ -168,6 +189,7 @@ __device__ __forceinline__ void visit_cell(const Geom& g, const Work& w, int c, 
                 continue;
             }
         }
+        EGG_STAT(a, kUsPairs, se - sb);
         for (int q = sb; q < se; q++) {
             float d2 = 0.f;
             for (int l = 0; l < d; l++) d2 = dist_step(__ldg(w.X + (size_t)l * g.ns + q), x[l], d2);
@@ -185,6 +207,7 @@ __device__ __forceinline__ void visit_cell(const Geom& g, const Work& w, int c, 
         a.N += cnt;
         a.partial_in += cnt;
     }
+    EGG_STAT(a, kUsPairsIn, cnt);
 }
 
 }  // namespace
@@ -260,6 +283,15 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
     a.N = 0;
     a.partial_in = 0;
     a.tab_err = false;
+#ifdef EGG_UPDATE_STATS
+    for (int k = 0; k < kUStats; k++) a.st[k] = 0;
+    {
+        // every lane takes part in the vote (a full-mask vote by one lane never completes)
+        const int ob0 = __shfl_sync(0xffffffffu, obase, 0);
+        const bool uniform = __all_sync(0xffffffffu, obase == ob0);
+        if (lane == 0 && !uniform) a.st[kUsLaneWarps] = 1;
+    }
+#endif
     const int own = w.cell_of[iv];
     const int own_cnt = w.cell_start[own + 1] - w.cell_start[own];
 
@@ -292,7 +324,10 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
         if (!border) viol = (N != own_cnt);
         else if (a.partial_in > 0) viol = true;
         else if (N == own_cnt) viol = false;
-        else viol = (N != half_count<D>(g, w, x, gi, obase, own, own_cnt));
+        else {
+            viol = (N != half_count<D>(g, w, x, gi, obase, own, own_cnt));
+            EGG_STAT(a, kUsHalfCount, 1);
+        }
         w.viol_orig[w.orig[i]] = viol ? 1 : 0;
         if (moved) {
             unsigned char* dcur = w.dirty[it & 1];
@@ -305,6 +340,20 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
         if (*f != 0) *f = 0;
     }
     if (a.tab_err) atomicOr(w.ctrl + kCtrlStatus, kErrTable);
+#ifdef EGG_UPDATE_STATS
+    if (valid) {
+        a.st[kUsPoints] += 1;
+        a.st[kUsNeighbors] += N;
+    } else {
+        for (int k = 0; k < kUStats; k++) if (k != kUsLaneWarps) a.st[k] = 0;  // shadow lanes
+    }
+    for (int k = 0; k < kUStats; k++) {
+        unsigned long long v = a.st[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0 && v) atomicAdd(w.ustats + k, v);
+    }
+#endif
 }
 
 template <int D>
@@ -312,11 +361,9 @@ __global__ void __launch_bounds__(128) k_update(Geom g, Work w, int* __restrict_
     update_body<D>(g, w, counts, blockIdx.x);
 }
 
-template <int D>
-__global__ void __launch_bounds__(128) kb_update(BatchArgs B, int skip) {
-    EGG_BATCH_ENTRY(B, skip);
-    (void)gx;
-    update_body<D>(g, w, nullptr, bx);
+template <int D, int T>
+__global__ void __launch_bounds__(T) kb_update(BatchArgs B) {
+    batch_for(B, [&](const Geom& g, const Work& w, int bx, int) { update_body<D>(g, w, nullptr, bx); });
 }
 
 #define EGG_DISPATCH_D(d, KERNEL, ...)                \
@@ -362,26 +409,46 @@ __device__ __forceinline__ void need_body(const Geom& g, const Work& w, int bx, 
 
 __global__ void k_need(Geom g, Work w) { need_body(g, w, blockIdx.x, gridDim.x); }
 
-__global__ void kb_need(BatchArgs B, int skip) {
-    EGG_BATCH_ENTRY(B, skip);
-    need_body(g, w, bx, gx);
+__global__ void kb_need(BatchArgs B) {
+    batch_for(B, [&](const Geom& g, const Work& w, int bx, int gx) { need_body(g, w, bx, gx); });
 }
 
 void launch_need(const Exec& ex, cudaStream_t st) {
     if (ex.batch())
-        kb_need<<<ex.blocks(kShapeCapOuter), 256, 0, st>>>(ex.args(kShapeCapOuter), ex.skip_done);
+        kb_need<<<ex.blocks(kShapeCapOuter, 256), 256, 0, st>>>(ex.args(kShapeCapOuter));
     else
-        k_need<<<ex.blocks(kShapeCapOuter), 256, 0, st>>>(*ex.g, *ex.w);
+        k_need<<<ex.blocks(kShapeCapOuter, 256), 256, 0, st>>>(*ex.g, *ex.w);
+}
+
+#define EGG_DISPATCH_DT(d, KERNEL, T, ...)            \
+    switch (d) {                                      \
+        case 1: KERNEL<1, T> __VA_ARGS__; break;      \
+        case 2: KERNEL<2, T> __VA_ARGS__; break;      \
+        case 3: KERNEL<3, T> __VA_ARGS__; break;      \
+        case 4: KERNEL<4, T> __VA_ARGS__; break;      \
+        case 5: KERNEL<5, T> __VA_ARGS__; break;      \
+        case 6: KERNEL<6, T> __VA_ARGS__; break;      \
+        case 8: KERNEL<8, T> __VA_ARGS__; break;      \
+        case 16: KERNEL<16, T> __VA_ARGS__; break;    \
+        default: KERNEL<0, T> __VA_ARGS__; break;     \
+    }
+
+template <int T>
+void launch_update_batch(const Exec& ex, size_t smem, cudaStream_t st) {
+    const int shape = T == 64 ? kShapeN64 : (T == 128 ? kShapeN128 : kShapeN256);
+    EGG_DISPATCH_DT(ex.d, kb_update, T, <<<ex.blocks(shape, T), T, smem, st>>>(ex.args(shape)));
 }
 
 void launch_update(const Exec& ex, int* counts, cudaStream_t st) {
-    const int threads = 128;
     const size_t smem = sizeof(float) * 3 * (2 * ex.table_k() + 1);
     if (ex.batch()) {
-        EGG_DISPATCH_D(ex.d, kb_update,
-                       <<<ex.blocks(kShapeN128), threads, smem, st>>>(ex.args(kShapeN128), ex.skip_done));
+        switch (ex.update_threads()) {
+            case 64: launch_update_batch<64>(ex, smem, st); break;
+            case 256: launch_update_batch<256>(ex, smem, st); break;
+            default: launch_update_batch<128>(ex, smem, st); break;
+        }
     } else {
-        EGG_DISPATCH_D(ex.d, k_update, <<<ex.blocks(kShapeN128), threads, smem, st>>>(*ex.g, *ex.w, counts));
+        EGG_DISPATCH_D(ex.d, k_update, <<<ex.blocks(kShapeN128, 128), 128, smem, st>>>(*ex.g, *ex.w, counts));
     }
 }
 

@@ -23,13 +23,19 @@ EGG_ERR_INTERNAL = -6
 
 # every symbol include/eggsync.h declares
 EXPORTS = ("egg_opts_default", "egg_sync_run", "egg_sync_step", "egg_sync_grid", "egg_sync_grid_noalloc",
-           "egg_status_str", "egg_last_error", "egg_release", "egg_abi_version")
+           "egg_sync_batch", "egg_status_str", "egg_last_error", "egg_release", "egg_abi_version",
+           "egg_update_counters")
+
+# egg_update_counters slots
+UPDATE_COUNTERS = ("points", "cells", "small_pass", "full", "tight_in", "tight_out", "groups_in", "groups_out",
+                   "pairs", "pairs_in", "lane_warps", "half_count", "neighbors")
 
 
 class EggOpts(C.Structure):
     _fields_ = [("max_iter", C.c_int32), ("loop", C.c_int32), ("stop_rule", C.c_int32),
                 ("order_param", C.c_int32), ("profile", C.c_int32), ("full_update", C.c_int32),
-                ("positions_out", C.c_void_p), ("labels_mode", C.c_int32), ("reserved", C.c_int32 * 7)]
+                ("positions_out", C.c_void_p), ("labels_mode", C.c_int32), ("batch_tune", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
 
 
 class EggStats(C.Structure):
@@ -40,6 +46,20 @@ class EggStats(C.Structure):
                 ("kernel_ms", C.c_float * 4), ("kernel_launches", C.c_int32 * 4), ("launches", C.c_int32),
                 ("order_param_lo", C.c_double), ("order_param_hi", C.c_double),
                 ("itr_order_param", C.POINTER(C.c_double))]
+
+
+class EggBatchItem(C.Structure):
+    _fields_ = [("x", C.c_void_p), ("n", C.c_int64), ("d", C.c_int32), ("eps", C.c_float),
+                ("labels", C.c_void_p), ("iterations", C.c_int32), ("converged", C.c_int32),
+                ("n_clusters", C.c_int32), ("status", C.c_int32)]
+
+
+class EggBatchStats(C.Structure):
+    _fields_ = [("loop_iterations", C.c_int32), ("groups", C.c_int32), ("launches", C.c_int32),
+                ("tuned", C.c_int32), ("update_threads", C.c_int32), ("blocks_per_sm", C.c_int32),
+                ("order", C.c_int32), ("reserved0", C.c_int32), ("workspace_bytes", C.c_int64),
+                ("total_ms", C.c_float), ("loop_ms", C.c_float), ("tune_ms", C.c_float),
+                ("itr_cap", C.c_int32), ("itr_ms", C.POINTER(C.c_float)), ("reserved", C.c_int32 * 2)]
 
 
 class EggError(RuntimeError):
@@ -79,6 +99,8 @@ def load():
     L.egg_sync_grid.restype = C.c_int
     L.egg_sync_grid_noalloc.argtypes = [vp, C.c_int64, C.c_int32, C.c_float, vp, vp, vp, C.POINTER(C.c_int32), vp]
     L.egg_sync_grid_noalloc.restype = C.c_int
+    L.egg_sync_batch.argtypes = [C.POINTER(EggBatchItem), C.c_int32, C.POINTER(EggOpts), C.POINTER(EggBatchStats), vp]
+    L.egg_sync_batch.restype = C.c_int
     L.egg_status_str.argtypes = [C.c_int]
     L.egg_status_str.restype = C.c_char_p
     L.egg_last_error.argtypes = []
@@ -87,6 +109,8 @@ def load():
     L.egg_release.restype = C.c_int
     L.egg_abi_version.argtypes = []
     L.egg_abi_version.restype = C.c_int
+    L.egg_update_counters.argtypes = [C.POINTER(C.c_int64), C.c_int32]
+    L.egg_update_counters.restype = C.c_int
     _lib = L
     return L
 

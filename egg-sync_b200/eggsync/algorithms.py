@@ -188,6 +188,64 @@ def egg_grid(D, eps: float):
     return order, cell_of, start[: M.value + 1].copy()
 
 
+def egg_sync_batch(instances, max_iter: int = 0, full_update: bool = False, tune: str = "auto",
+                   loop: str = "graph", labels_out=None):
+    """Run many instances in one batched call (one CUDA graph for all).
+
+    ``instances``: sequence of (D, eps) pairs; each D is an n x d float32
+    numpy array or torch tensor (host or CUDA), sizes and dimensions may
+    differ.  ``labels_out`` (optional) gives one preallocated int32 buffer per
+    instance.  ``tune``: "auto" (autotune once per workload, cached), "off"
+    (default configuration) or "again".  Returns (list of (labels, info),
+    batch info).  Every instance's labels and iteration count equal those of
+    ``egg_sync`` on it alone."""
+    L = _lib.load()
+    m = len(instances)
+    items = (_lib.EggBatchItem * m)()
+    keep = []
+    outs = []
+    dev = None
+    stream = None
+    for k, (D, eps) in enumerate(instances):
+        ptr, n, d, kp, dv, st = _prepare(D)
+        keep.append(kp)
+        if dv is not None:
+            if dev is not None and dv != dev:
+                raise ValueError("all device inputs of a batch must be on one device")
+            dev, stream = dv, st
+        out = labels_out[k] if labels_out is not None else np.empty(n, np.int32)
+        outs.append(out)
+        it = items[k]
+        it.x, it.n, it.d, it.eps = ptr, n, d, float(eps)
+        it.labels = _out_ptr(out, n, np.int32, "labels_out[%d]" % k)
+    opts = EggOpts()
+    L.egg_opts_default(C.byref(opts))
+    opts.max_iter = int(max_iter)
+    opts.full_update = 1 if full_update else 0
+    opts.batch_tune = {"auto": 0, "off": 1, "again": 2}[tune]
+    opts.loop = {"graph": 0, "host": 1}[loop]
+    stats = _lib.EggBatchStats()
+    cap = opts.max_iter if opts.max_iter > 0 else 1000
+    itr = (C.c_float * cap)()
+    stats.itr_ms = C.cast(itr, C.POINTER(C.c_float))
+    stats.itr_cap = cap
+    with _DeviceGuard(dev):
+        check(L.egg_sync_batch(items, m, C.byref(opts), C.byref(stats), C.c_void_p(stream) if stream else None))
+    del keep
+    results = []
+    for k in range(m):
+        it = items[k]
+        if it.status < 0:
+            raise EggError(it.status, "instance %d" % k)
+        results.append((outs[k], {"iterations": int(it.iterations), "converged": bool(it.converged),
+                                  "n_clusters": int(it.n_clusters), "status": int(it.status)}))
+    binfo = {f: getattr(stats, f) for f, _ in _lib.EggBatchStats._fields_
+             if not f.startswith("reserved") and f not in ("itr_ms", "itr_cap")}
+    binfo = {k: (float(v) if isinstance(v, float) else int(v)) for k, v in binfo.items()}
+    binfo["itr_ms"] = [float(itr[i]) for i in range(min(stats.loop_iterations, cap))]
+    return results, binfo
+
+
 class _Impl:
     """Stand-in for the reference's JIT module object ``impl``."""
 
@@ -210,4 +268,4 @@ def EGG_SynC(D, eps, lam=DEFAULT_LAMBDA):
     return impl.EGG_SynC_wrapper(D, eps, lam)
 
 
-__all__ = ["EGG_SynC", "impl", "egg_sync", "egg_step", "egg_grid", "EggError", "DEFAULT_LAMBDA"]
+__all__ = ["EGG_SynC", "impl", "egg_sync", "egg_sync_batch", "egg_step", "egg_grid", "EggError", "DEFAULT_LAMBDA"]

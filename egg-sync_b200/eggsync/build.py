@@ -43,11 +43,18 @@ def _compile(src: Path, obj: Path, extra):
     return r.stderr
 
 
-def build(force: bool = False, verbose: bool = False, extra=()) -> Path:
-    LIBDIR.mkdir(exist_ok=True)
+def build(force: bool = False, verbose: bool = False, extra=(), stats: bool = False) -> Path:
+    """Build libeggsync.so, or with ``stats`` libeggsync_stats.so: the same
+    kernels with the update kernel's interaction counters compiled in
+    (-DEGG_UPDATE_STATS), for measurement only."""
+    objdir = LIBDIR / "stats" if stats else LIBDIR
+    lib = LIBDIR / "libeggsync_stats.so" if stats else LIB
+    if stats:
+        extra = tuple(extra) + ("-DEGG_UPDATE_STATS",)
+    objdir.mkdir(parents=True, exist_ok=True)
     headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(INCLUDE.glob("*.h"))
     srcs = sources()
-    objs = [LIBDIR / (s.stem + ".o") for s in srcs]
+    objs = [objdir / (s.stem + ".o") for s in srcs]
     todo = [(s, o) for s, o in zip(srcs, objs) if force or _stale(o, [s] + headers)]
     if todo:
         with cf.ThreadPoolExecutor(max_workers=min(8, len(todo))) as ex:
@@ -56,19 +63,19 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> Path:
                 msg = f.result()
                 if verbose and msg:
                     sys.stderr.write(msg)
-    if force or todo or _stale(LIB, objs):
-        tmp = LIB.with_suffix(".so.tmp%d" % os.getpid())
+    if force or todo or _stale(lib, objs):
+        tmp = lib.with_suffix(".so.tmp%d" % os.getpid())
         # the CUDA runtime is linked statically: the library does not depend
         # on which libcudart the host process (e.g. torch) happens to load
         cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", str(tmp)] + [str(o) for o in objs]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (r.stdout[-4000:], r.stderr[-4000:]))
-        os.replace(tmp, LIB)
-    return LIB
+        os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":
     v = "-v" in sys.argv
     extra = ["-Xptxas", "-v"] if v else []
-    print(build(force="--force" in sys.argv, verbose=v, extra=extra))
+    print(build(force="--force" in sys.argv, verbose=v, extra=extra, stats="--stats" in sys.argv))

@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define EGG_SYNC_ABI_VERSION 1
+#define EGG_SYNC_ABI_VERSION 2
 
 typedef enum egg_status {
     EGG_OK = 0,
@@ -48,7 +48,10 @@ typedef struct egg_opts {
     float *positions_out; /* optional n x d buffer (host or device): final positions, input order */
     int32_t labels_mode;  /* 0 = GPU union-find over the points of each final cell (default),
                              1 = direct per-cell labelling; both give identical labels */
-    int32_t reserved[7];
+    int32_t batch_tune;   /* egg_sync_batch only: 0 = autotune the launch configuration once per
+                             workload signature (cached for later calls), 1 = default configuration,
+                             2 = tune again */
+    int32_t reserved[6];
 } egg_opts;
 
 typedef struct egg_stats {
@@ -130,6 +133,51 @@ int egg_sync_grid(const float *x, int64_t n, int32_t d, float eps, int32_t *orde
 int egg_sync_grid_noalloc(const float *x, int64_t n, int32_t d, float eps, int32_t *order, int32_t *cell_of,
                           int32_t *cell_start, int32_t *n_cells, void *stream);
 
+/* One instance of a batched run (egg_sync_batch). */
+typedef struct egg_batch_item {
+    const float *x;       /* n x d float32, row-major, host or device */
+    int64_t n;
+    int32_t d;
+    float eps;
+    int32_t *labels;      /* n int32 (host or device), as egg_sync_run's labels */
+    int32_t iterations;   /* out: loop iterations of this instance */
+    int32_t converged;    /* out: 1 when the reference's flag ended its loop */
+    int32_t n_clusters;   /* out: final cells holding more than one point */
+    int32_t status;       /* out: EGG_OK, EGG_MAX_ITER, or EGG_ERR_INPUT (NaN/Inf in x, labels not written) */
+} egg_batch_item;
+
+typedef struct egg_batch_stats {
+    int32_t loop_iterations;  /* iterations of the batch loop (the largest instance's count) */
+    int32_t groups;           /* instance groups: one per dimension d present */
+    int32_t launches;         /* kernels the call launched, graph replays included */
+    int32_t tuned;            /* 1 when this call ran the autotuner */
+    int32_t update_threads;   /* configuration used: update kernel block size */
+    int32_t blocks_per_sm;    /* persistent blocks per SM of a 256-thread kernel */
+    int32_t order;            /* 0 = input order, 1 = instances by decreasing size */
+    int32_t reserved0;
+    int64_t workspace_bytes;
+    float total_ms;           /* device time of the call (CUDA events), tuning excluded */
+    float loop_ms;            /* device time of the batch loop */
+    float tune_ms;            /* host time spent autotuning (0 when cached or off) */
+    int32_t itr_cap;          /* entries of itr_ms */
+    float *itr_ms;            /* optional caller array: device time of each batch-loop iteration */
+    int32_t reserved[2];
+} egg_batch_stats;
+
+/* Run EGG-SynC on many independent instances at once: datasets of uneven
+ * size and dimension, eps sweeps.  No counterpart in the reference, whose
+ * wrapper runs one instance per call (src/maps/map.cpp:31-33).  Every
+ * instance gets exactly the labels and iteration count that egg_sync_run
+ * gives it alone.  All instances iterate inside one CUDA graph (one
+ * conditional while loop, one persistent launch per kernel for all
+ * instances of a dimension); finished instances drop out of the launches.
+ * opts: max_iter, full_update and batch_tune are used; stop_rule and
+ * order_param must be 0.  1 <= count <= 1024.  stats may be NULL.
+ * Returns EGG_OK when every instance was processed (see each item's status),
+ * else an error for the whole call. */
+int egg_sync_batch(egg_batch_item *items, int32_t count, const egg_opts *opts, egg_batch_stats *stats,
+                   void *stream);
+
 /* Human-readable name of a status value. */
 const char *egg_status_str(int status);
 
@@ -141,6 +189,17 @@ int egg_release(void);
 
 /* EGG_SYNC_ABI_VERSION of the loaded library. */
 int egg_abi_version(void);
+
+/* Interaction counters of the update kernel summed over the last
+ * egg_sync_run: point updates computed, candidate cells examined, cells
+ * passing the reference's small box test, cells aggregated as fully covered,
+ * cells aggregated / skipped by their points' tight box, 32-point groups
+ * aggregated / skipped, point-pair distance tests, pairs within eps, warps
+ * that walked the stencil lane by lane, half-count evaluations, sum of
+ * |N(p)| (in this order; 16 slots).  Only the stats build
+ * (libeggsync_stats.so) collects them; it writes min(cap, 16) values and
+ * returns 16.  The normal build returns 0.  No counterpart in the reference. */
+int egg_update_counters(int64_t *out, int32_t cap);
 
 #ifdef __cplusplus
 }

@@ -33,7 +33,10 @@ def test_exports_every_declared_symbol(eggsync_lib):
 
 
 def test_abi_version_and_status_names(eggsync_lib):
-    assert eggsync_lib.egg_abi_version() == 1
+    assert eggsync_lib.egg_abi_version() == 2
+    # the normal build collects no interaction counters
+    buf = (C.c_int64 * 16)()
+    assert eggsync_lib.egg_update_counters(buf, 16) == 0
     assert eggsync_lib.egg_status_str(0) == b"EGG_OK"
     assert eggsync_lib.egg_status_str(-4) == b"EGG_ERR_CUDA"
     assert eggsync_lib.egg_status_str(12345) == b"EGG_UNKNOWN_STATUS"
@@ -41,14 +44,22 @@ def test_abi_version_and_status_names(eggsync_lib):
 
 def test_struct_layout_matches_header(tmp_path):
     src = tmp_path / "sz.c"
-    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "eggsync.h"\n'
-                   'int main(){printf("%zu %zu %zu %zu %zu\\n", sizeof(egg_opts), sizeof(egg_stats),'
-                   ' offsetof(egg_stats, stage_ms), offsetof(egg_stats, itr_ms), offsetof(egg_stats, itr_cap));}\n')
+    fields = [("egg_opts", _lib.EggOpts, ["positions_out", "labels_mode", "batch_tune"]),
+              ("egg_stats", _lib.EggStats, ["stage_ms", "itr_ms", "itr_cap", "itr_order_param"]),
+              ("egg_batch_item", _lib.EggBatchItem, ["n", "eps", "labels", "status"]),
+              ("egg_batch_stats", _lib.EggBatchStats, ["workspace_bytes", "total_ms", "tune_ms", "itr_ms"])]
+    body = "".join('printf("%%zu\\n", sizeof(%s));' % t + "".join(
+        'printf("%%zu\\n", offsetof(%s, %s));' % (t, f) for f in fs) for t, _, fs in fields)
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "eggsync.h"\nint main(){%s}\n' % body)
     exe = tmp_path / "sz"
     subprocess.run(["gcc", "-I", str(REPO / "include"), str(src), "-o", str(exe)], check=True)
     vals = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
-    assert vals == [C.sizeof(_lib.EggOpts), C.sizeof(_lib.EggStats), _lib.EggStats.stage_ms.offset,
-                    _lib.EggStats.itr_ms.offset, _lib.EggStats.itr_cap.offset]
+    want = []
+    for _, S, fs in fields:
+        want.append(C.sizeof(S))
+        want.extend(getattr(S, f).offset for f in fs)
+    assert vals == want
+    assert C.sizeof(_lib.EggOpts) == 64
 
 
 def _run(L, x, n, d, eps, labels):
@@ -75,6 +86,28 @@ def test_argument_errors(eggsync_lib):
     assert _run(L, xp, 10, 2, 1e-6, lp) == _lib.EGG_ERR_GEOMETRY
     flags = np.zeros(2, np.int32)
     assert L.egg_sync_step(None, 10, 2, 0.05, xp, None, C.c_void_p(flags.ctypes.data), None) == _lib.EGG_ERR_ARG
+
+
+def test_batch_argument_errors(eggsync_lib):
+    L = eggsync_lib
+    x = np.zeros((10, 2), np.float32)
+    lab = np.zeros(10, np.int32)
+    items = (_lib.EggBatchItem * 2)()
+    for it in items:
+        it.x, it.n, it.d, it.eps, it.labels = x.ctypes.data, 10, 2, 0.05, lab.ctypes.data
+    assert L.egg_sync_batch(None, 2, None, None, None) == _lib.EGG_ERR_ARG
+    assert L.egg_sync_batch(items, 0, None, None, None) == _lib.EGG_ERR_ARG
+    assert L.egg_sync_batch(items, 1025, None, None, None) == _lib.EGG_ERR_ARG
+    items[1].eps = 5.0
+    assert L.egg_sync_batch(items, 2, None, None, None) == _lib.EGG_ERR_GEOMETRY
+    assert L.egg_last_error().startswith(b"item 1:")
+    items[1].eps = 0.05
+    items[0].labels = None
+    assert L.egg_sync_batch(items, 2, None, None, None) == _lib.EGG_ERR_ARG
+    items[0].labels = lab.ctypes.data
+    opts = _lib.EggOpts()
+    opts.stop_rule = 1
+    assert L.egg_sync_batch(items, 2, C.byref(opts), None, None) == _lib.EGG_ERR_ARG
 
 
 def test_python_front_end_rejects_bad_input(eggsync_lib):
