@@ -27,6 +27,14 @@ enum : int {
     kErrStencil = 4,
 };
 
+// The update kernel's point-by-point walks read a candidate point's
+// coordinates and its sin / 1 - cos offsets as whole 16-byte records when
+// d <= kPackDims: pack_w(d) float4 of coordinates, pack_s(d) float4 of the
+// 2d offsets, zero-padded.
+constexpr int kPackDims = 8;
+__host__ __device__ constexpr int pack_w(int d) { return (d + 3) / 4; }
+__host__ __device__ constexpr int pack_s(int d) { return (2 * d + 3) / 4; }
+
 // Per-instance geometry, exactly as the reference computes it
 // (src/algorithms/EGG_SynC.cu:1249-1260, 1430, 563, 779, 1045).
 struct Geom {
@@ -60,8 +68,10 @@ struct Work {
     // points, in the current cell-sorted order
     float* X;          // [d][ns] positions (current grid)
     float* Xn;         // [d][ns] positions after the update (same order as X)
-    float* sd;         // [d][ns] sin(delta), delta = x - cell corner
-    float* md;         // [d][ns] 1 - cos(delta) (= 2 sin^2(delta/2))
+    float* sd;         // [d][ns] sin(delta), delta = x - cell corner (d > kPackDims)
+    float* md;         // [d][ns] 1 - cos(delta) (= 2 sin^2(delta/2))  (d > kPackDims)
+    float4* xp;        // [ns][pack_w(d)] positions packed per point (d <= kPackDims)
+    float4* smp;       // [ns][pack_s(d)] sin(delta) then 1 - cos(delta), packed per point (d <= kPackDims)
     float* qlo;        // [d][ns] eps/2-ball extremes (extra check)
     float* qhi;        // [d][ns]
     float* ulo;        // [d][ns] per cell: union of its points' eps/2-ball extremes

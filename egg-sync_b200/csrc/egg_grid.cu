@@ -371,6 +371,15 @@ __device__ __forceinline__ void cell_sums_body(const Geom& g, const Work& w, int
         if (((ce - 1) >> 5) - (cs >> 5) > 2) w.big_list[atomicAdd(w.ctrl + kCtrlBigCount, 1)] = c;
         else w.span_list[atomicAdd(w.ctrl + kCtrlSpanCount, 1)] = c;
     }
+    constexpr bool kPacked = D >= 1 && D <= kPackDims;
+    constexpr int PW = kPacked ? pack_w(D) : 1, PS = kPacked ? pack_s(D) : 1;
+    float pk_x[4 * PW], pk_s[4 * PS];
+    if constexpr (kPacked) {
+#pragma unroll
+        for (int k = 0; k < 4 * PW; k++) pk_x[k] = 0.f;
+#pragma unroll
+        for (int k = 0; k < 4 * PS; k++) pk_s[k] = 0.f;
+    }
     for (int l = 0; l < d; l++) {
         float s = 0.f, m = 0.f, x = 0.f;
         if (valid) {
@@ -382,8 +391,14 @@ __device__ __forceinline__ void cell_sums_body(const Geom& g, const Work& w, int
             sincosf(0.5f * delta, &sh, &ch);
             s = 2.0f * sh * ch;
             m = 2.0f * sh * sh;
-            w.sd[(size_t)l * g.ns + i] = s;
-            w.md[(size_t)l * g.ns + i] = m;
+            if constexpr (kPacked) {
+                pk_x[l] = x;
+                pk_s[l] = s;
+                pk_s[d + l] = m;
+            } else {
+                w.sd[(size_t)l * g.ns + i] = s;
+                w.md[(size_t)l * g.ns + i] = m;
+            }
         }
         TwoSum vs{s, 0.f}, vm{m, 0.f};
         float mn = x, mx = x;
@@ -427,6 +442,15 @@ __device__ __forceinline__ void cell_sums_body(const Geom& g, const Work& w, int
                 w.gpart[wp_idx(3, l, d, rec, nw, warp)] = mx;
             }
         }
+    }
+    if constexpr (kPacked) {
+        if (!valid) return;
+#pragma unroll
+        for (int k = 0; k < PW; k++)
+            w.xp[(size_t)i * PW + k] = make_float4(pk_x[4 * k], pk_x[4 * k + 1], pk_x[4 * k + 2], pk_x[4 * k + 3]);
+#pragma unroll
+        for (int k = 0; k < PS; k++)
+            w.smp[(size_t)i * PS + k] = make_float4(pk_s[4 * k], pk_s[4 * k + 1], pk_s[4 * k + 2], pk_s[4 * k + 3]);
     }
 }
 

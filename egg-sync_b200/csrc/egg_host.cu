@@ -147,8 +147,11 @@ size_t layout_work(const Geom& g, int max_iter, char* base, Work& w, float** xin
     };
     add((void**)&w.X, 4 * d * ns);
     add((void**)&w.Xn, 4 * d * ns);
-    add((void**)&w.sd, 4 * d * ns);
-    add((void**)&w.md, 4 * d * ns);
+    const bool packed = d <= kPackDims;
+    add((void**)&w.sd, packed ? 0 : 4 * d * ns);
+    add((void**)&w.md, packed ? 0 : 4 * d * ns);
+    add((void**)&w.xp, packed ? 16 * (size_t)pack_w(d) * ns : 0);
+    add((void**)&w.smp, packed ? 16 * (size_t)pack_s(d) * ns : 0);
     add((void**)&w.qlo, 4 * d * ns);
     add((void**)&w.qhi, 4 * d * ns);
     add((void**)&w.ulo, 4 * d * ns);

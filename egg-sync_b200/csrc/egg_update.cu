@@ -190,15 +190,53 @@ __device__ __forceinline__ void visit_cell(const Geom& g, const Work& w, int c, 
             }
         }
         EGG_STAT(a, kUsPairs, se - sb);
-        for (int q = sb; q < se; q++) {
-            float d2 = 0.f;
-            for (int l = 0; l < d; l++) d2 = dist_step(__ldg(w.X + (size_t)l * g.ns + q), x[l], d2);
-            if (d2 <= g.t_eps) {
-                for (int l = 0; l < d; l++) {
-                    as[l] += __ldg(w.sd + (size_t)l * g.ns + q);
-                    am[l] += __ldg(w.md + (size_t)l * g.ns + q);
+        if constexpr (D >= 1 && D <= kPackDims) {
+            // packed records: one or two 16-byte loads per candidate point
+            constexpr int PW = pack_w(D > 0 ? D : 1), PS = pack_s(D > 0 ? D : 1);
+            const float4* xp = w.xp + (size_t)sb * PW;
+            const float4* sp = w.smp + (size_t)sb * PS;
+            for (int q = sb; q < se; q++, xp += PW, sp += PS) {
+                float xq[4 * PW];
+#pragma unroll
+                for (int k = 0; k < PW; k++) {
+                    const float4 v = __ldg(xp + k);
+                    xq[4 * k] = v.x;
+                    xq[4 * k + 1] = v.y;
+                    xq[4 * k + 2] = v.z;
+                    xq[4 * k + 3] = v.w;
                 }
-                cnt++;
+                float d2 = 0.f;
+#pragma unroll
+                for (int l = 0; l < DM; l++) d2 = dist_step(xq[l], x[l], d2);
+                if (d2 <= g.t_eps) {
+                    float v[4 * PS];
+#pragma unroll
+                    for (int k = 0; k < PS; k++) {
+                        const float4 t = __ldg(sp + k);
+                        v[4 * k] = t.x;
+                        v[4 * k + 1] = t.y;
+                        v[4 * k + 2] = t.z;
+                        v[4 * k + 3] = t.w;
+                    }
+#pragma unroll
+                    for (int l = 0; l < DM; l++) {
+                        as[l] += v[l];
+                        am[l] += v[DM + l];
+                    }
+                    cnt++;
+                }
+            }
+        } else {
+            for (int q = sb; q < se; q++) {
+                float d2 = 0.f;
+                for (int l = 0; l < d; l++) d2 = dist_step(__ldg(w.X + (size_t)l * g.ns + q), x[l], d2);
+                if (d2 <= g.t_eps) {
+                    for (int l = 0; l < d; l++) {
+                        as[l] += __ldg(w.sd + (size_t)l * g.ns + q);
+                        am[l] += __ldg(w.md + (size_t)l * g.ns + q);
+                    }
+                    cnt++;
+                }
             }
         }
     }
