@@ -18,6 +18,12 @@ from positions to converged labels.
   on its launching stream in a profiled run.
 * cpu_baseline: the reference's own CPU SynC (src/algorithms/SynC.cpp, built
   from its sources into oracle/_ref) on a bounded sample of the same workload.
+* learned (N = 1): the same workload with the learned warm start
+  (eggsync/models/warm_d3.npz, unverified): time, iterations and the
+  adjusted Rand index of its partition against the plain run's.
+* batched_sweep (N = 1): 64 datasets x 8 eps (512 runs) in one batched call
+  against 512 sequential calls, with an identity check of all labels.
+  --no-extra skips these two legs.
 
 With --gpus N (under torchrun) every rank runs its own replica (the loop does
 not shard); value is the max over ranks.  --impl reference times the
@@ -54,6 +60,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-extra", action="store_true", help="skip the learned and batched-sweep legs")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--cpu-sample", type=int, default=0, help="points in the CPU-baseline sample (0 = auto)")
@@ -245,6 +252,8 @@ def run_ours(args, rank, local, world, pg):
 
     # profiled run: every kernel group bracketed by CUDA events on its stream
     _, pinfo = egg_sync(Xd, eps, labels_out=lab_d, profile=True)
+    learned = learned_leg(args, timed, Xd, eps, lab_d, dev) if world == 1 and not args.no_extra else None
+    sweep = batched_sweep(dev) if world == 1 and not args.no_extra else None
 
     ms = statistics.mean(dev_times)
     ms_e2e = statistics.mean(e2e_times)
@@ -296,7 +305,87 @@ def run_ours(args, rank, local, world, pg):
         "clocks": clocks,
         "cpu_baseline": cpu_baseline(X, eps, iters, sample),
     }
+    if learned is not None:
+        line["learned"] = learned
+    if sweep is not None:
+        line["batched_sweep"] = sweep
     return line
+
+
+def ari(a, b):
+    """Adjusted Rand index of two labelings (every label value is a group)."""
+    a = np.asarray(a, np.int64)
+    b = np.asarray(b, np.int64)
+    _, ai = np.unique(a, return_inverse=True)
+    _, bi = np.unique(b, return_inverse=True)
+    pairs = ai * (bi.max() + 1) + bi
+    _, nij = np.unique(pairs, return_counts=True)
+    comb = lambda x: (x.astype(np.float64) * (x - 1) / 2).sum()  # noqa: E731
+    sij = comb(nij)
+    sa = comb(np.bincount(ai))
+    sb = comb(np.bincount(bi))
+    expected = sa * sb / comb(np.array([len(a)]))
+    mx = (sa + sb) / 2
+    return 1.0 if mx == expected else float((sij - expected) / (mx - expected))
+
+
+def learned_leg(args, timed, Xd, eps, lab_plain, dev):
+    """The learned warm start on the same workload: unverified time, its
+    iterations and the agreement of its partition with the plain run's."""
+    import torch
+
+    from eggsync import egg_sync, warm
+
+    model = warm.default_model(Xd.shape[1])
+    if model is None:
+        return {"unavailable": "no trained warm-start model for d = %d" % Xd.shape[1]}
+    lab_w = torch.empty_like(lab_plain)
+    for _ in range(max(args.warmup, 1)):
+        egg_sync(Xd, eps, labels_out=lab_w, warm_start=model)
+    times, (_, info) = timed(lambda: egg_sync(Xd, eps, labels_out=lab_w, warm_start=model))
+    a, b = lab_plain.cpu().numpy(), lab_w.cpu().numpy()
+    _, vinfo = egg_sync(Xd, eps, labels_out=lab_w, warm_start=model, warm_verify=True)
+    return {"value": statistics.mean(times) / 1000.0, "unit": "s", "iterations": info["iterations"],
+            "warm_ms": info["warm_ms"], "ari_vs_plain": ari(a, b),
+            "same_partition_as_plain": bool(vinfo["warm_same"]), "verified_fallback": bool(vinfo["warm_fallback"]),
+            "model": "eggsync/models/warm_d3.npz (K=%d, min_count %d)" % (model.k_steps, model.min_count),
+            "note": "unverified warm start; with warm_verify the call returns the plain partition when they differ"}
+
+
+def batched_sweep(dev):
+    """C4: 64 datasets x 8 eps (512 runs) in one egg_sync_batch call against
+    512 sequential egg_sync calls; device inputs and outputs, wall clock
+    around each call after a synchronize."""
+    import time
+
+    import torch
+
+    from eggsync import data, egg_sync, egg_sync_batch
+
+    inst = [(torch.from_numpy(c["X"]).to(dev), e) for c in data.c4(0) for e in c["eps"]]
+    ob = [torch.empty(len(x), dtype=torch.int32, device=dev) for x, _ in inst]
+    os_ = [torch.empty(len(x), dtype=torch.int32, device=dev) for x, _ in inst]
+    res, bi = egg_sync_batch(inst, labels_out=ob)  # tunes once (cached)
+    tb = []
+    for _ in range(3):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        res, bi = egg_sync_batch(inst, labels_out=ob)
+        torch.cuda.synchronize(dev)
+        tb.append(time.perf_counter() - t0)
+    for x, e in inst[:8]:
+        egg_sync(x, e)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    sres = [egg_sync(x, e, labels_out=o) for (x, e), o in zip(inst, os_)]
+    torch.cuda.synchronize(dev)
+    ts = time.perf_counter() - t0
+    same = all(torch.equal(a, b) for a, b in zip(ob, os_)) and all(
+        r[1]["iterations"] == q[1]["iterations"] for r, q in zip(res, sres))
+    return {"workload": "c4: 64 datasets (n 1k-200k, d in {2,3,5}) x 8 eps in [0.01, 0.08], 512 runs",
+            "batched_s": min(tb), "sequential_s": ts, "speedup": ts / min(tb), "identical_to_sequential": same,
+            "loop_iterations": bi["loop_iterations"], "launch_config": {k: bi[k] for k in (
+                "update_threads", "blocks_per_sm", "order")}}
 
 
 def run_reference(args, rank, world):

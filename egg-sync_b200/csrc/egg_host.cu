@@ -28,6 +28,7 @@
 #include "egg_common.cuh"
 #include "egg_host_common.h"
 #include "egg_kernels.h"
+#include "egg_mlp.h"
 
 namespace egg {
 
@@ -244,6 +245,8 @@ struct Instance {
     float* xin = nullptr;                  // staging for host input (n*d)
     int max_iter = 0;
     size_t used = 0;
+    mlp::Buffers warm;                     // learned warm start
+    cudaEvent_t wev[2] = {};
     // graph cache
     cudaGraphExec_t exec = nullptr;
     std::vector<char> graph_key;
@@ -476,6 +479,15 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
     prepare(I, g, max_iter);
     load_input(I, x, opts.full_update ? 1 : 0);
     check_status_bits(I);
+    float warm_ms = 0.f;
+    if (opts.warm_start) {
+        // displace the input by the network's prediction; the loop starts there
+        if (!I.wev[0])
+            for (auto& e : I.wev) EGG_CHECK(cudaEventCreate(&e));
+        EGG_CHECK(cudaEventRecord(I.wev[0], I.st));
+        mlp::warm_start(*opts.warm_start, I.w.Xn, (size_t)g.ns, g.n, g.d, eps, I.warm, I.st);
+        EGG_CHECK(cudaEventRecord(I.wev[1], I.st));
+    }
     EGG_CHECK(cudaEventRecord(I.ev[1], I.st));
 
     float kms[4] = {0, 0, 0, 0};
@@ -593,12 +605,89 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
         const int per_iter = build_l + 10 + ((g.order_mode == 2 || g.stop_rule == 1) ? 2 : 0);
         const int final_l = build_l + (opts.labels_mode == 1 ? 1 : 4) + (g.order_mode == 1 ? 4 : 0) +
                             (opts.positions_out ? 1 : 0);
-        stats->launches = 2 + iters * per_iter + final_l;
+        stats->launches = 2 + iters * per_iter + final_l + (opts.warm_start ? 10 : 0);
+        stats->warm_started = opts.warm_start ? 1 : 0;
+        stats->warm_fallback = 0;
+        stats->warm_same = 0;
+        if (opts.warm_start) EGG_CHECK(cudaEventElapsedTime(&warm_ms, I.wev[0], I.wev[1]));
+        stats->warm_ms = warm_ms;
     }
     if (I.h_ctrl[kCtrlStatus] & ~kErrNonFinite)
         throw ArgError{EGG_ERR_INTERNAL, "kernel consistency check failed (status bits " +
                                              std::to_string(I.h_ctrl[kCtrlStatus]) + ")"};
     return converged ? EGG_OK : EGG_MAX_ITER;
+}
+
+// identical partitions: -1 in the same places and a bijection between the
+// other label values
+bool same_partition(const std::vector<int32_t>& a, const std::vector<int32_t>& b) {
+    if (a.size() != b.size()) return false;
+    std::map<int32_t, int32_t> ab, ba;
+    for (size_t i = 0; i < a.size(); i++) {
+        if ((a[i] < 0) != (b[i] < 0)) return false;
+        if (a[i] < 0) continue;
+        auto x = ab.emplace(a[i], b[i]);
+        if (x.first->second != b[i]) return false;
+        auto y = ba.emplace(b[i], a[i]);
+        if (y.first->second != a[i]) return false;
+    }
+    return true;
+}
+
+// Warm start with verification: run from the network's positions and from
+// the input, return the warm run when both give the same partition, else
+// the plain run (the fallback).
+int run_verified(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_opts* opts_in, int32_t* labels,
+                 egg_stats* stats, void* stream) {
+    if (!x || !labels) throw ArgError{EGG_ERR_ARG, "x and labels must not be NULL"};
+    if (n < 1 || n > (int64_t)0x7ffffff0 / 4 || d < 1 || d > kMaxDims) throw ArgError{EGG_ERR_ARG, "n or d out of range"};
+    const egg_opts opts = *opts_in;
+    const int cap = stats && stats->itr_cap > 0 ? stats->itr_cap : 0;
+    struct Leg {
+        std::vector<int32_t> lab;
+        std::vector<float> pos, itr;
+        std::vector<double> itr_r;
+        egg_stats st;
+        int status;
+    } leg[2];
+    for (int k = 0; k < 2; k++) {
+        Leg& L = leg[k];
+        L.lab.resize((size_t)n);
+        if (opts.positions_out) L.pos.resize((size_t)n * d);
+        L.itr.resize(std::max(cap, 1));
+        L.itr_r.resize(2 * (size_t)std::max(cap, 1));
+        memset(&L.st, 0, sizeof(L.st));
+        L.st.itr_ms = stats && stats->itr_ms ? L.itr.data() : nullptr;
+        L.st.itr_order_param = stats && stats->itr_order_param ? L.itr_r.data() : nullptr;
+        L.st.itr_cap = cap;
+        egg_opts o = opts;
+        o.warm_verify = 0;
+        if (k == 1) o.warm_start = nullptr;
+        o.positions_out = opts.positions_out ? L.pos.data() : nullptr;
+        L.status = run(x, n, d, eps, lam, &o, L.lab.data(), &L.st, stream);
+    }
+    const bool same = same_partition(leg[0].lab, leg[1].lab);
+    Leg& R = leg[same ? 0 : 1];
+    EGG_CHECK(cudaMemcpy(labels, R.lab.data(), 4 * (size_t)n, cudaMemcpyDefault));
+    if (opts.positions_out)
+        EGG_CHECK(cudaMemcpy(opts.positions_out, R.pos.data(), 4 * (size_t)n * d, cudaMemcpyDefault));
+    if (stats) {
+        float* itr = stats->itr_ms;
+        double* itr_r = stats->itr_order_param;
+        const int icap = stats->itr_cap;
+        *stats = R.st;
+        stats->itr_ms = itr;
+        stats->itr_order_param = itr_r;
+        stats->itr_cap = icap;
+        const int m = std::min(R.st.iterations, icap);
+        if (itr && m > 0) memcpy(itr, R.itr.data(), 4 * (size_t)m);
+        if (itr_r && m > 0) memcpy(itr_r, R.itr_r.data(), 16 * (size_t)m);
+        stats->warm_same = same ? 1 : 0;
+        stats->warm_fallback = same ? 0 : 1;
+        stats->warm_started = same ? 1 : 0;
+        stats->warm_ms = leg[0].st.warm_ms;
+    }
+    return R.status;
 }
 
 int step(const float* x, int64_t n, int32_t d, float eps, float* x_next, int32_t* counts, int32_t* flags,
@@ -773,12 +862,16 @@ int grid_noalloc(const float* x, int64_t n, int32_t d, float eps, int32_t* order
 
 int release() {
     release_batch();
+    mlp::release_all();
     for (auto& kv : g_inst) {
         Instance* I = kv.second;
         int cur = 0;
         cudaGetDevice(&cur);
         cudaSetDevice(I->dev);
         destroy_graph(*I);
+        mlp::release(I->warm);
+        for (auto e : I->wev)
+            if (e) cudaEventDestroy(e);
         if (I->base) cudaFree(I->base);
         if (I->h_ctrl) cudaFreeHost(I->h_ctrl);
         if (I->h_stamps) cudaFreeHost(I->h_stamps);
@@ -808,7 +901,11 @@ __attribute__((visibility("default"))) void egg_opts_default(egg_opts* opts) {
 __attribute__((visibility("default"))) int egg_sync_run(const float* x, int64_t n, int32_t d, float eps, float lam,
                                                         const egg_opts* opts, int32_t* labels, egg_stats* stats,
                                                         void* stream) {
-    return egg::guarded([&] { return egg::run(x, n, d, eps, lam, opts, labels, stats, stream); });
+    return egg::guarded([&] {
+        if (opts && opts->warm_start && opts->warm_verify)
+            return egg::run_verified(x, n, d, eps, lam, opts, labels, stats, stream);
+        return egg::run(x, n, d, eps, lam, opts, labels, stats, stream);
+    });
 }
 
 __attribute__((visibility("default"))) int egg_sync_step(const float* x, int64_t n, int32_t d, float eps,

@@ -24,18 +24,30 @@ EGG_ERR_INTERNAL = -6
 # every symbol include/eggsync.h declares
 EXPORTS = ("egg_opts_default", "egg_sync_run", "egg_sync_step", "egg_sync_grid", "egg_sync_grid_noalloc",
            "egg_sync_batch", "egg_status_str", "egg_last_error", "egg_release", "egg_abi_version",
-           "egg_update_counters")
+           "egg_update_counters", "egg_mlp_feature_dim", "egg_mlp_features", "egg_mlp_forward", "egg_mlp_grad",
+           "egg_mlp_train")
 
 # egg_update_counters slots
 UPDATE_COUNTERS = ("points", "cells", "small_pass", "full", "tight_in", "tight_out", "groups_in", "groups_out",
                    "pairs", "pairs_in", "lane_warps", "half_count", "neighbors")
 
 
+class EggMlp(C.Structure):
+    _fields_ = [("d", C.c_int32), ("d_in", C.c_int32), ("hidden", C.c_int32), ("k_steps", C.c_int32),
+                ("min_count", C.c_int32), ("reserved0", C.c_int32), ("w1", C.c_void_p), ("b1", C.c_void_p), ("w2", C.c_void_p), ("b2", C.c_void_p),
+                ("w3", C.c_void_p), ("b3", C.c_void_p)]
+
+
+class EggMlpTrainOpts(C.Structure):
+    _fields_ = [("epochs", C.c_int32), ("batch", C.c_int32), ("lr", C.c_float), ("reserved0", C.c_int32),
+                ("seed", C.c_int64)]
+
+
 class EggOpts(C.Structure):
     _fields_ = [("max_iter", C.c_int32), ("loop", C.c_int32), ("stop_rule", C.c_int32),
                 ("order_param", C.c_int32), ("profile", C.c_int32), ("full_update", C.c_int32),
                 ("positions_out", C.c_void_p), ("labels_mode", C.c_int32), ("batch_tune", C.c_int32),
-                ("reserved", C.c_int32 * 6)]
+                ("warm_start", C.c_void_p), ("warm_verify", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class EggStats(C.Structure):
@@ -45,7 +57,8 @@ class EggStats(C.Structure):
                 ("total_ms", C.c_float), ("itr_ms", C.POINTER(C.c_float)), ("itr_cap", C.c_int32),
                 ("kernel_ms", C.c_float * 4), ("kernel_launches", C.c_int32 * 4), ("launches", C.c_int32),
                 ("order_param_lo", C.c_double), ("order_param_hi", C.c_double),
-                ("itr_order_param", C.POINTER(C.c_double))]
+                ("itr_order_param", C.POINTER(C.c_double)), ("warm_started", C.c_int32),
+                ("warm_fallback", C.c_int32), ("warm_ms", C.c_float), ("warm_same", C.c_int32)]
 
 
 class EggBatchItem(C.Structure):
@@ -111,6 +124,17 @@ def load():
     L.egg_abi_version.restype = C.c_int
     L.egg_update_counters.argtypes = [C.POINTER(C.c_int64), C.c_int32]
     L.egg_update_counters.restype = C.c_int
+    L.egg_mlp_feature_dim.argtypes = [C.c_int32]
+    L.egg_mlp_feature_dim.restype = C.c_int
+    L.egg_mlp_features.argtypes = [vp, C.c_int64, C.c_int32, C.c_float, vp]
+    L.egg_mlp_features.restype = C.c_int
+    L.egg_mlp_forward.argtypes = [C.POINTER(EggMlp), vp, C.c_int64, vp]
+    L.egg_mlp_forward.restype = C.c_int
+    L.egg_mlp_grad.argtypes = [C.POINTER(EggMlp), vp, vp, C.c_int64, C.POINTER(EggMlp), C.POINTER(C.c_double)]
+    L.egg_mlp_grad.restype = C.c_int
+    L.egg_mlp_train.argtypes = [C.POINTER(EggMlp), vp, vp, C.c_int64, C.POINTER(EggMlpTrainOpts),
+                                C.POINTER(C.c_double)]
+    L.egg_mlp_train.restype = C.c_int
     _lib = L
     return L
 

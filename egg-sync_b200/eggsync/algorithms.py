@@ -92,7 +92,7 @@ def _out_ptr(buf, n, dtype_np, what):
 def egg_sync(D, eps: float, lam: float = DEFAULT_LAMBDA, max_iter: int = 0, loop: str = "graph",
              labels_out=None, profile: bool = False, full_update: bool = False,
              positions_out=None, stop_rule: str = "flag", order_param: int = 0,
-             labels_mode: str = "union_find") -> Tuple[object, dict]:
+             labels_mode: str = "union_find", warm_start=None, warm_verify: bool = False) -> Tuple[object, dict]:
     """Run EGG-SynC; return (int32 labels, stats dict).
 
     ``labels_out`` may be a preallocated int32 numpy array or torch tensor
@@ -105,7 +105,10 @@ def egg_sync(D, eps: float, lam: float = DEFAULT_LAMBDA, max_iter: int = 0, loop
     positions.  ``stop_rule`` "flag" is the reference EGG-SynC's convergence
     test; "lambda" stops once the certified lower bound of the FP64 local
     order parameter reaches ``lam``.  ``order_param`` 1 reports the order
-    parameter of the final positions, 2 that of every iteration."""
+    parameter of the final positions, 2 that of every iteration.
+    ``warm_start`` (an ``eggsync.warm.Model``, d <= 3) displaces the input by
+    the network's prediction before the plain loop; ``warm_verify`` also runs
+    the plain loop from the input and returns it when the partitions differ."""
     L = _lib.load()
     ptr, n, d, keep, dev, stream = _prepare(D)
     if labels_out is None:
@@ -122,6 +125,11 @@ def egg_sync(D, eps: float, lam: float = DEFAULT_LAMBDA, max_iter: int = 0, loop
     opts.labels_mode = {"union_find": 0, "cells": 1}[labels_mode]
     if positions_out is not None:
         opts.positions_out = _out_ptr(positions_out, n * d, np.float32, "positions_out")
+    mlp = None
+    if warm_start is not None:
+        mlp = warm_start.struct()
+        opts.warm_start = C.addressof(mlp)
+        opts.warm_verify = 1 if warm_verify else 0
     stats = EggStats()
     cap = opts.max_iter if opts.max_iter > 0 else 1000
     itr = (C.c_float * cap)()
@@ -153,7 +161,12 @@ def egg_sync(D, eps: float, lam: float = DEFAULT_LAMBDA, max_iter: int = 0, loop
         "itr_order_param": [(float(itr_r[2 * k]), float(itr_r[2 * k + 1]))
                             for k in range(min(stats.iterations, cap))] if (order_param == 2 or
                                                                              stop_rule == "lambda") else [],
+        "warm_started": bool(stats.warm_started),
+        "warm_fallback": bool(stats.warm_fallback),
+        "warm_same": bool(stats.warm_same),
+        "warm_ms": float(stats.warm_ms),
     }
+    del mlp
     return labels_out, info
 
 

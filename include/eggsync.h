@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define EGG_SYNC_ABI_VERSION 2
+#define EGG_SYNC_ABI_VERSION 3
 
 typedef enum egg_status {
     EGG_OK = 0,
@@ -31,6 +31,32 @@ typedef enum egg_status {
     EGG_ERR_NO_DEVICE = -5,  /* no CUDA device */
     EGG_ERR_INTERNAL = -6    /* an internal consistency check failed */
 } egg_status;
+
+/* A trained warm-start network (see egg_mlp_train): 3 dense layers,
+ * d_in -> hidden -> hidden -> d, ReLU after the two hidden layers.  It maps
+ * a point's features (egg_mlp_features) to its displacement over the next
+ * k_steps iterations of the plain loop, in units of eps.  Weights are
+ * float32 row-major [in][out], host or device memory. */
+typedef struct egg_mlp {
+    int32_t d;        /* point dimension, 1..3 */
+    int32_t d_in;     /* d + 3^d (1 + 2d): 192 for d = 3 */
+    int32_t hidden;   /* 128 */
+    int32_t k_steps;  /* iterations the network was trained to predict (informational) */
+    int32_t min_count; /* only points with at least this many points in their 3^d coarse cells are
+                          displaced; sparse points keep their input positions */
+    int32_t reserved0;
+    float *w1, *b1;   /* [d_in][hidden], [hidden] */
+    float *w2, *b2;   /* [hidden][hidden], [hidden] */
+    float *w3, *b3;   /* [hidden][d], [d] */
+} egg_mlp;
+
+typedef struct egg_mlp_train_opts {
+    int32_t epochs;
+    int32_t batch;    /* rows per Adam step, 16..65536 */
+    float lr;         /* peak learning rate (cosine decay to 5% of it) */
+    int32_t reserved0;
+    int64_t seed;     /* shuffling seed */
+} egg_mlp_train_opts;
 
 typedef struct egg_opts {
     int32_t max_iter;     /* iteration cap; 0 = default (1000).  The reference has none. */
@@ -51,7 +77,11 @@ typedef struct egg_opts {
     int32_t batch_tune;   /* egg_sync_batch only: 0 = autotune the launch configuration once per
                              workload signature (cached for later calls), 1 = default configuration,
                              2 = tune again */
-    int32_t reserved[6];
+    const egg_mlp *warm_start;  /* optional (egg_sync_run, d <= 3): displace the input by the network's
+                                   prediction, then run the plain loop from there to convergence */
+    int32_t warm_verify;  /* with warm_start: also run the plain loop from the input and return its
+                             result (stats->warm_fallback = 1) when the two partitions differ */
+    int32_t reserved[3];
 } egg_opts;
 
 typedef struct egg_stats {
@@ -77,6 +107,10 @@ typedef struct egg_stats {
     double order_param_hi;
     double *itr_order_param; /* optional caller array of 2*itr_cap doubles: [lo, hi] per iteration
                                 (opts->order_param == 2 or stop_rule == 1) */
+    int32_t warm_started;  /* 1 when the returned result started from the network's positions */
+    int32_t warm_fallback; /* 1 when warm_verify found a different partition and returned the plain run */
+    float warm_ms;         /* device time of the warm start (features + network + displacement) */
+    int32_t warm_same;     /* warm_verify: 1 when the two partitions were identical */
 } egg_stats;
 
 /* Fill *opts with the defaults (all zero). */
@@ -177,6 +211,34 @@ typedef struct egg_batch_stats {
  * else an error for the whole call. */
 int egg_sync_batch(egg_batch_item *items, int32_t count, const egg_opts *opts, egg_batch_stats *stats,
                    void *stream);
+
+/* Learned warm start (no counterpart in the reference).  Width of one
+ * feature row: feat_dim(d) = d + 3^d (1 + 2d) rounded up to a multiple of
+ * 16 (192 for d = 3); -1 for d outside 1..3. */
+int egg_mlp_feature_dim(int32_t d);
+
+/* Features of n points x (row-major n x d, host or device): feats receives
+ * n rows of egg_mlp_feature_dim(d) float32 values (zero padded).  A coarse
+ * grid of side eps; per point its offset in its coarse cell and, for each of
+ * the 3^d cells around it, log1p(count)/8, centroid minus point and the
+ * spread of the offsets (eps units). */
+int egg_mlp_features(const float *x, int64_t n, int32_t d, float eps, float *feats);
+
+/* The network on n feature rows (BF16 tensor-core inference, FP32
+ * accumulation): out receives n x d displacements in eps units. */
+int egg_mlp_forward(const egg_mlp *m, const float *feats, int64_t n, float *out);
+
+/* Mean squared error of the network on n rows (FP32) and its gradient:
+ * grad's weight arrays (float32, caller-owned) receive d loss / d weight. */
+int egg_mlp_grad(const egg_mlp *m, const float *feats, const float *targets, int64_t n, egg_mlp *grad,
+                 double *loss);
+
+/* Train m in place (FP32, Adam, minibatches of opts->batch rows, shuffled
+ * with opts->seed) on n rows of features and target displacements (n x d,
+ * eps units).  epoch_loss (optional, opts->epochs entries) receives each
+ * epoch's mean squared error. */
+int egg_mlp_train(egg_mlp *m, const float *feats, const float *targets, int64_t n,
+                  const egg_mlp_train_opts *opts, double *epoch_loss);
 
 /* Human-readable name of a status value. */
 const char *egg_status_str(int status);

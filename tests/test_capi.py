@@ -33,7 +33,7 @@ def test_exports_every_declared_symbol(eggsync_lib):
 
 
 def test_abi_version_and_status_names(eggsync_lib):
-    assert eggsync_lib.egg_abi_version() == 2
+    assert eggsync_lib.egg_abi_version() == 3
     # the normal build collects no interaction counters
     buf = (C.c_int64 * 16)()
     assert eggsync_lib.egg_update_counters(buf, 16) == 0
@@ -44,8 +44,12 @@ def test_abi_version_and_status_names(eggsync_lib):
 
 def test_struct_layout_matches_header(tmp_path):
     src = tmp_path / "sz.c"
-    fields = [("egg_opts", _lib.EggOpts, ["positions_out", "labels_mode", "batch_tune"]),
-              ("egg_stats", _lib.EggStats, ["stage_ms", "itr_ms", "itr_cap", "itr_order_param"]),
+    fields = [("egg_opts", _lib.EggOpts, ["positions_out", "labels_mode", "batch_tune", "warm_start",
+                                           "warm_verify"]),
+              ("egg_stats", _lib.EggStats, ["stage_ms", "itr_ms", "itr_cap", "itr_order_param", "warm_ms",
+                                            "warm_same"]),
+              ("egg_mlp", _lib.EggMlp, ["min_count", "w1", "b3"]),
+              ("egg_mlp_train_opts", _lib.EggMlpTrainOpts, ["lr", "seed"]),
               ("egg_batch_item", _lib.EggBatchItem, ["n", "eps", "labels", "status"]),
               ("egg_batch_stats", _lib.EggBatchStats, ["workspace_bytes", "total_ms", "tune_ms", "itr_ms"])]
     body = "".join('printf("%%zu\\n", sizeof(%s));' % t + "".join(

@@ -1,0 +1,106 @@
+"""GPU tests of the learned warm start: features, BF16 tensor-core inference
+and FP32 training gradients against the CPU oracle (oracle/mlp_oracle.py);
+the warm-started loop returns the plain loop's partition (verified, with
+fallback)."""
+import numpy as np
+import pytest
+
+import mlp_oracle as M
+from eggsync import data, egg_sync, warm
+
+pytestmark = pytest.mark.gpu
+
+
+def small3d(n=20000, seed=0):
+    return data.c5(seed, n=n)
+
+
+def random_model(d, seed=0, scale=1.0):
+    m = warm.Model(d, seed=seed)
+    if scale != 1.0:
+        for k in m.w:
+            m.w[k] *= scale
+    rng = np.random.default_rng(seed + 1)
+    m.w["b1"][:] = rng.standard_normal(m.w["b1"].shape) * 0.05
+    m.w["b2"][:] = rng.standard_normal(m.w["b2"].shape) * 0.05
+    return m
+
+
+@pytest.mark.parametrize("d", [1, 2, 3])
+def test_features_match_oracle(d):
+    rng = np.random.default_rng(d)
+    X = data.min_max_normalize(rng.standard_normal((5000, d)) * 0.1 + 0.5)
+    X[:5] = 1.0  # upper edge
+    X[5:10] = 0.0
+    for eps in (0.02, 0.05):
+        g = warm.features(X, eps)
+        o = M.features(X, eps)
+        assert g.shape == o.shape == (len(X), M.feature_width(d))
+        assert np.abs(g - o).max() <= 2e-6
+
+
+def test_forward_bf16_tensor_cores_match_oracle():
+    c = small3d()
+    f = warm.features(c["X"], c["eps"])
+    m = random_model(3)
+    y = warm.forward(m, f)
+    ref = M.forward(m.w, f, 3, emulate_bf16=True)
+    ref32 = M.forward(m.w, f, 3)
+    scale = np.abs(ref).max()
+    assert np.abs(y - ref).max() <= 1e-2 * scale
+    assert np.abs(y - ref32).max() <= 5e-2 * scale
+    # partial last tile
+    y7 = warm.forward(m, f[:37])
+    assert np.array_equal(y7, y[:37])
+
+
+def test_gradient_matches_oracle():
+    c = small3d(4000)
+    f = warm.features(c["X"], c["eps"])[:256]
+    rng = np.random.default_rng(2)
+    t = rng.standard_normal((256, 3)).astype(np.float32) * 0.3
+    m = random_model(3, seed=3)
+    loss, g = warm.grad(m, f, t)
+    rloss, rg = M.grad(m.w, f, t, 3)
+    assert abs(loss - rloss) <= 1e-5 * rloss
+    for k in M.NAMES:
+        err = np.linalg.norm(g[k] - rg[k]) / max(np.linalg.norm(rg[k]), 1e-30)
+        assert err <= 1e-4, k
+
+
+def test_training_reduces_loss_and_is_deterministic():
+    c = small3d(8000)
+    f, t = warm.trajectory_pair(c["X"], c["eps"], 8)
+    a, b = random_model(3, seed=4), random_model(3, seed=4)
+    la = warm.train(a, f, t, epochs=4, batch=512, lr=1e-3, seed=7)
+    lb = warm.train(b, f, t, epochs=4, batch=512, lr=1e-3, seed=7)
+    assert la == lb
+    assert all(np.array_equal(a.w[k], b.w[k]) for k in M.NAMES)
+    assert la[-1] < la[0]
+
+
+def test_warm_start_verified_returns_plain_partition():
+    c = small3d()
+    X, eps = c["X"], c["eps"]
+    plain, pinfo = egg_sync(X, eps)
+    m = warm.default_model(3)
+    if m is None:
+        m = random_model(3, scale=0.01)
+    lab, info = egg_sync(X, eps, warm_start=m, warm_verify=True)
+    from oracle import same_partition
+    assert same_partition(lab, plain)
+    assert info["warm_same"] != info["warm_fallback"]
+    # an unverified warm start runs from the displaced positions
+    lab2, info2 = egg_sync(X, eps, warm_start=m)
+    assert info2["warm_started"] and info2["converged"] and info2["warm_ms"] > 0
+
+
+def test_bad_network_falls_back():
+    c = small3d()
+    X, eps = c["X"], c["eps"]
+    plain, pinfo = egg_sync(X, eps)
+    bad = random_model(3, seed=9, scale=30.0)  # displacements of many eps
+    lab, info = egg_sync(X, eps, warm_start=bad, warm_verify=True)
+    assert info["warm_fallback"] and not info["warm_same"]
+    assert np.array_equal(lab, plain)
+    assert info["iterations"] == pinfo["iterations"]
