@@ -52,6 +52,10 @@ L2_FLUSH_BYTES = 256 << 20
 # Iterations the reference EGG semantics take on this workload (measured by
 # the plain GPU path; used only to extrapolate the CPU baseline).
 C5_ITERATIONS = 191
+# DRAM bytes (read + written) of one update launch on this workload, mean over
+# the 191 launches of a run, from one ncu capture of the dram__bytes counters
+# (python bench.py --profile-run under ncu -k regex:k_update).
+UPDATE_DRAM_BYTES_PER_LAUNCH = 22.85e6
 
 
 def parse():
@@ -295,7 +299,9 @@ def run_ours(args, rank, local, world, pg):
                 "d2h_bytes_per_step": int(n * 4)},
         "gpu_launches": int(info["launches"]) * args.steps,
         "roofline": {"bound": "hbm", "kernel": "k_update", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": UPDATE_DRAM_BYTES_PER_LAUNCH,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, mean over the 191 "
+                                       "update launches of one run of this workload",
                      "peak_source": peak_kind, "launch_ms": upd_ms,
                      "launches": pinfo["kernel_launches"]["update"],
                      "algorithmic_bytes_per_launch": ub,

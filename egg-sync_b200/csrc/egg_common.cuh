@@ -163,9 +163,11 @@ enum : int {
     kUsGroupsOut,      // 32-point groups skipped
     kUsPairs,          // point-pair distance tests
     kUsPairsIn,        // ... within eps
-    kUsLaneWarps,      // warps that walked the stencil lane by lane
+    kUsLaneWarps,      // warps whose lanes span several outer cells
     kUsHalfCount,      // border points that needed the half count
     kUsNeighbors,      // sum of |N(p)|
+    kUsCyclesShared,   // SM cycles of the candidate walk, warps whose lanes share one outer cell
+    kUsCyclesLane,     // SM cycles of the candidate walk, warps whose lanes span several outer cells
     kUStats = 16
 };
 

@@ -333,8 +333,18 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
     const int own = w.cell_of[iv];
     const int own_cnt = w.cell_start[own + 1] - w.cell_start[own];
 
+#ifdef EGG_UPDATE_STATS
+    const long long t_walk0 = clock64();
+#endif
     for_candidates(g, w, gi, obase, lane, d,
                    [&](int c) { visit_cell<D>(g, w, c, x, gi, a, Ts, Tc, Tm, K, TW); });
+#ifdef EGG_UPDATE_STATS
+    {
+        const long long dt = clock64() - t_walk0;
+        const long long warp_dt = __reduce_max_sync(0xffffffffu, (unsigned)min(dt, 0x7fffffffLL));
+        if (lane == 0) a.st[a.st[kUsLaneWarps] ? kUsCyclesLane : kUsCyclesShared] += (unsigned)warp_dt;
+    }
+#endif
 
     const int N = a.N;
     const float fN = (float)N;

@@ -29,7 +29,7 @@ EXPORTS = ("egg_opts_default", "egg_sync_run", "egg_sync_step", "egg_sync_grid",
 
 # egg_update_counters slots
 UPDATE_COUNTERS = ("points", "cells", "small_pass", "full", "tight_in", "tight_out", "groups_in", "groups_out",
-                   "pairs", "pairs_in", "lane_warps", "half_count", "neighbors")
+                   "pairs", "pairs_in", "lane_warps", "half_count", "neighbors", "cycles_shared", "cycles_lane")
 
 
 class EggMlp(C.Structure):

@@ -258,7 +258,9 @@ int egg_abi_version(void);
  * cells aggregated / skipped by their points' tight box, 32-point groups
  * aggregated / skipped, point-pair distance tests, pairs within eps, warps
  * that walked the stencil lane by lane, half-count evaluations, sum of
- * |N(p)| (in this order; 16 slots).  Only the stats build
+ * |N(p)|, SM cycles of the candidate walk in warps whose lanes share one
+ * outer cell and in warps that walked lane by lane (in this order; 16
+ * slots).  Only the stats build
  * (libeggsync_stats.so) collects them; it writes min(cap, 16) values and
  * returns 16.  The normal build returns 0.  No counterpart in the reference. */
 int egg_update_counters(int64_t *out, int32_t cap);
