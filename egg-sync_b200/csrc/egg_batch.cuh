@@ -100,13 +100,17 @@ __device__ __forceinline__ void batch_for(const BatchArgs& B, F&& body) {
     __shared__ Geom s_g;
     __shared__ Work s_w;
     __shared__ int s_boff[kMaxBatch + 1];
+    __shared__ int s_act[kMaxBatch];
     __shared__ int s_info[4];  // list entry, its first virtual block, its block count, entry loaded
+    // the offset table and the list in one round of loads after the list length
     const int na = *B.nact;
-    const int tot = B.boff[na];
-    if ((int)blockIdx.x >= tot) return;
-    for (int t = threadIdx.x; t <= na; t += blockDim.x) s_boff[t] = B.boff[t];
+    for (int t = threadIdx.x; t <= na; t += blockDim.x) {
+        s_boff[t] = B.boff[t];
+        if (t < na) s_act[t] = B.active[t];
+    }
     if (threadIdx.x == 0) s_info[3] = -1;
     __syncthreads();
+    const int tot = s_boff[na];
     for (int vb = blockIdx.x; vb < tot; vb += gridDim.x) {
         if (threadIdx.x == 0) {
             int lo = 0, hi = na - 1;
@@ -120,7 +124,7 @@ __device__ __forceinline__ void batch_for(const BatchArgs& B, F&& body) {
         }
         __syncthreads();
         if (s_info[0] != s_info[3]) {
-            const int inst = B.active[s_info[0]];
+            const int inst = s_act[s_info[0]];
             const int* sg = reinterpret_cast<const int*>(B.geoms + inst);
             const int* sw = reinterpret_cast<const int*>(B.works + inst);
             int* dg = reinterpret_cast<int*>(&s_g);

@@ -163,6 +163,18 @@ __global__ void __launch_bounds__(1024) k_batch_ctl(CtlArgs a, int phase, cudaGr
     }
 }
 
+// Opens the conditional node of every group that still has active
+// instances (run at the start of each loop iteration).
+constexpr int kMaxGroups = 16;
+struct GateHandles {
+    cudaGraphConditionalHandle h[kMaxGroups];
+};
+
+__global__ void k_batch_gate(const int* nact, int ngroups, GateHandles hs) {
+    const int k = threadIdx.x;
+    if (k < ngroups) cudaGraphSetConditional(hs.h[k], nact[k] > 0 ? 1u : 0u);
+}
+
 __global__ void k_batch_reset(const Work* works, int count, int max_iter, int full_update) {
     const int i = blockIdx.x;
     if (i >= count) return;
@@ -419,20 +431,25 @@ void set_tables(Plan& P, const Config& c) {
 }
 
 // one iteration of every group, then the control kernel
+// one iteration of group k's instances
+void enqueue_group(Plan& P, int k, cudaStream_t st) {
+    Group& gr = P.groups[k];
+    const Exec ex = batched(gr.act, gr.d);
+    launch_build(ex, st);
+    launch_cell_sums(ex, st);
+    launch_need(ex, st);
+    launch_update(ex, nullptr, st);
+    kb_mark_extra<<<ex.blocks(kShapeOne, 32), 32, 0, st>>>(ex.args(kShapeOne));
+    launch_extra_check(ex, st);
+}
+
 void enqueue_iteration(State& S, Plan& P, cudaGraphConditionalHandle h, int in_graph) {
     const int G = (int)P.groups.size();
     if (G > 1) EGG_CHECK(cudaEventRecord(S.fork, S.st));
     for (int k = 0; k < G; k++) {
-        Group& gr = P.groups[k];
         cudaStream_t st = G > 1 ? S.gstreams[k] : S.st;
         if (G > 1) EGG_CHECK(cudaStreamWaitEvent(st, S.fork, 0));
-        const Exec ex = batched(gr.act, gr.d);
-        launch_build(ex, st);
-        launch_cell_sums(ex, st);
-        launch_need(ex, st);
-        launch_update(ex, nullptr, st);
-        kb_mark_extra<<<ex.blocks(kShapeOne, 32), 32, 0, st>>>(ex.args(kShapeOne));
-        launch_extra_check(ex, st);
+        enqueue_group(P, k, st);
         if (G > 1) {
             EGG_CHECK(cudaEventRecord(S.gjoins[k], st));
             EGG_CHECK(cudaStreamWaitEvent(S.st, S.gjoins[k], 0));
@@ -483,19 +500,73 @@ cudaGraphExec_t get_graph(State& S, Plan& P, const Config& c) {
         e = cudaGraphAddNode(&node, graph, nullptr, 0, &p);
         if (e == cudaSuccess) body = p.conditional.phGraph_out[0];
     }
-    if (e == cudaSuccess)
-        e = cudaStreamBeginCaptureToGraph(S.st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess) {
-        bool ok = true;
-        try {
-            enqueue_iteration(S, P, h, 1);
-        } catch (const CudaError& ce) {
-            ok = false;
-            e = ce.code;
+    const int G = (int)P.groups.size();
+    if (e == cudaSuccess && G <= kMaxGroups) {
+        // body: gate kernel -> one conditional IF node per group (siblings, so
+        // the groups run concurrently and an idle group launches nothing) ->
+        // control kernel
+        GateHandles hs = {};
+        for (int k = 0; k < G && e == cudaSuccess; k++)
+            e = cudaGraphConditionalHandleCreate(&hs.h[k], body, 1, 0);
+        cudaGraphNode_t gate = nullptr;
+        if (e == cudaSuccess) {
+            int ng = G;
+            void* gargs[] = {&P.d_nact, &ng, &hs};
+            cudaKernelNodeParams kp = {};
+            kp.func = (void*)k_batch_gate;
+            kp.gridDim = dim3(1);
+            kp.blockDim = dim3(32);
+            kp.kernelParams = gargs;
+            e = cudaGraphAddKernelNode(&gate, body, nullptr, 0, &kp);
         }
-        cudaGraph_t captured = nullptr;
-        const cudaError_t e2 = cudaStreamEndCapture(S.st, &captured);
-        if (ok) e = e2;
+        std::vector<cudaGraphNode_t> ifs(G);
+        for (int k = 0; k < G && e == cudaSuccess; k++) {
+            cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+            cp.conditional.handle = hs.h[k];
+            cp.conditional.type = cudaGraphCondTypeIf;
+            cp.conditional.size = 1;
+            e = cudaGraphAddNode(&ifs[k], body, &gate, 1, &cp);
+            if (e != cudaSuccess) break;
+            e = cudaStreamBeginCaptureToGraph(S.st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) break;
+            bool ok = true;
+            try {
+                enqueue_group(P, k, S.st);
+            } catch (const CudaError& ce) {
+                ok = false;
+                e = ce.code;
+            }
+            cudaGraph_t captured = nullptr;
+            const cudaError_t e2 = cudaStreamEndCapture(S.st, &captured);
+            if (ok) e = e2;
+        }
+        if (e == cudaSuccess) {
+            CtlArgs a = ctl_args(P);
+            int phase = 1, in_graph = 1;
+            void* cargs[] = {&a, &phase, &h, &in_graph};
+            cudaKernelNodeParams kp = {};
+            kp.func = (void*)k_batch_ctl;
+            kp.gridDim = dim3(1);
+            kp.blockDim = dim3(1024);
+            kp.kernelParams = cargs;
+            cudaGraphNode_t ctl;
+            e = cudaGraphAddKernelNode(&ctl, body, ifs.data(), G, &kp);
+        }
+    } else if (e == cudaSuccess) {
+        e = cudaStreamBeginCaptureToGraph(S.st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            bool ok = true;
+            try {
+                enqueue_iteration(S, P, h, 1);
+            } catch (const CudaError& ce) {
+                ok = false;
+                e = ce.code;
+            }
+            cudaGraph_t captured = nullptr;
+            const cudaError_t e2 = cudaStreamEndCapture(S.st, &captured);
+            if (ok) e = e2;
+        }
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
     if (graph) cudaGraphDestroy(graph);
@@ -689,9 +760,21 @@ int enqueue_prologue(State& S, Plan& P, int max_iter) {
     return launches + 1;
 }
 
-int per_iteration_launches(const Plan& P) {
-    int l = 1;  // control
-    for (const Group& gr : P.groups) l += 3 * gr.act.max_passes + 6 + 2 + 1 + 1 + 1 + 3;
+// kernels of one group's iteration: build, cell sums (2), need, update,
+// mark, extra check (3)
+int group_launches(const Group& gr) { return 3 * gr.act.max_passes + 6 + 2 + 1 + 1 + 1 + 3; }
+
+// Kernels of the loop: gate and control every iteration, and each group's
+// kernels in the iterations where it had active instances (the largest
+// iteration count among its instances; an idle group's conditional node
+// launches nothing).
+long long loop_launches(const Plan& P, int loop_iters, const std::vector<int>& res) {
+    long long l = 2LL * loop_iters;
+    for (const Group& gr : P.groups) {
+        int m = 0;
+        for (int pos = gr.begin; pos < gr.end; pos++) m = std::max(m, res[5 * (size_t)pos]);
+        l += (long long)m * group_launches(gr);
+    }
     return l;
 }
 
@@ -820,7 +903,7 @@ int run_batch(egg_batch_item* items, int count, const egg_opts* opts_in, egg_bat
     EGG_CHECK(cudaEventRecord(S.ev[0], S.st));
     int launches = enqueue_prologue(S, P, P.max_iter);
     EGG_CHECK(cudaEventRecord(S.ev[1], S.st));
-    enqueue_loop(S, P, cfg, opts.loop == 1);
+    const bool graph_loop = enqueue_loop(S, P, cfg, opts.loop == 1) < 0;
     EGG_CHECK(cudaEventRecord(S.ev[2], S.st));
     // final grid and labels of every instance (EGG_SynC.cu:1503-1522)
     for (Group& gr : P.groups) {
@@ -866,7 +949,12 @@ int run_batch(egg_batch_item* items, int count, const egg_opts* opts_in, egg_bat
         memset(stats, 0, sizeof(*stats));
         stats->loop_iterations = loop_iters;
         stats->groups = (int)P.groups.size();
-        stats->launches = launches + loop_iters * per_iteration_launches(P);
+        long long ll = loop_launches(P, loop_iters, res);
+        if (!graph_loop) {  // host-driven loop: every group launches in every iteration, no gate
+            ll = loop_iters;
+            for (const Group& gr : P.groups) ll += (long long)loop_iters * group_launches(gr);
+        }
+        stats->launches = (int32_t)std::min<long long>(0x7fffffff, launches + ll);
         stats->tuned = tuned_now ? 1 : 0;
         stats->update_threads = cfg.update_threads;
         stats->blocks_per_sm = cfg.occ;
