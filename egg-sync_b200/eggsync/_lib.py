@@ -25,7 +25,7 @@ EGG_ERR_INTERNAL = -6
 EXPORTS = ("egg_opts_default", "egg_sync_run", "egg_sync_step", "egg_sync_grid", "egg_sync_grid_noalloc",
            "egg_sync_batch", "egg_status_str", "egg_last_error", "egg_release", "egg_abi_version",
            "egg_update_counters", "egg_mlp_feature_dim", "egg_mlp_features", "egg_mlp_forward", "egg_mlp_grad",
-           "egg_mlp_train")
+           "egg_mlp_train", "egg_minmax_normalize", "egg_simple_sync_run")
 
 # egg_update_counters slots
 UPDATE_COUNTERS = ("points", "cells", "small_pass", "full", "tight_in", "tight_out", "groups_in", "groups_out",
@@ -124,6 +124,11 @@ def load():
     L.egg_abi_version.restype = C.c_int
     L.egg_update_counters.argtypes = [C.POINTER(C.c_int64), C.c_int32]
     L.egg_update_counters.restype = C.c_int
+    L.egg_simple_sync_run.argtypes = [vp, C.c_int64, C.c_int32, C.c_float, C.c_float, C.c_int32, vp, vp,
+                                      C.POINTER(EggStats), vp]
+    L.egg_simple_sync_run.restype = C.c_int
+    L.egg_minmax_normalize.argtypes = [vp, C.c_int64, C.c_int32, vp, vp, vp, vp]
+    L.egg_minmax_normalize.restype = C.c_int
     L.egg_mlp_feature_dim.argtypes = [C.c_int32]
     L.egg_mlp_feature_dim.restype = C.c_int
     L.egg_mlp_features.argtypes = [vp, C.c_int64, C.c_int32, C.c_float, vp]

@@ -259,6 +259,55 @@ def egg_sync_batch(instances, max_iter: int = 0, full_update: bool = False, tune
     return results, binfo
 
 
+def simple_sync(D, eps: float, lam: float = DEFAULT_LAMBDA, max_iter: int = 0, labels_out=None,
+                positions_out=None):
+    """Brute-force GPU SynC (simple_GPU_SynC.cu semantics): (int32 labels, info).
+    ``positions_out`` (optional n x d float32) receives the final positions."""
+    L = _lib.load()
+    ptr, n, d, keep, dev, stream = _prepare(D)
+    if labels_out is None:
+        labels_out = np.empty(n, np.int32)
+    lptr = _out_ptr(labels_out, n, np.int32, "labels_out")
+    pptr = _out_ptr(positions_out, n * d, np.float32, "positions_out") if positions_out is not None else None
+    stats = EggStats()
+    cap = max_iter if max_iter > 0 else 100
+    itr = (C.c_float * cap)()
+    stats.itr_ms = C.cast(itr, C.POINTER(C.c_float))
+    stats.itr_cap = cap
+    with _DeviceGuard(dev):
+        st = check(L.egg_simple_sync_run(C.c_void_p(ptr), n, d, float(eps), float(lam), int(max_iter),
+                                         C.c_void_p(lptr), C.c_void_p(pptr) if pptr else None, C.byref(stats),
+                                         C.c_void_p(stream) if stream else None))
+    del keep
+    return labels_out, {"status": int(st), "iterations": int(stats.iterations), "converged": bool(stats.converged),
+                        "n_clusters": int(stats.n_clusters), "r_local": float(stats.order_param),
+                        "itr_ms": [float(itr[i]) for i in range(min(stats.iterations, cap))],
+                        "stage_ms": [float(v) for v in stats.stage_ms], "total_ms": float(stats.total_ms),
+                        "workspace_bytes": int(stats.workspace_bytes)}
+
+
+def normalize(D, out=None):
+    """Per-dimension min-max normalisation on the GPU (python/data.py:100-103
+    semantics, float32).  D: n x d float32 numpy array or torch tensor (host
+    or CUDA); the result has D's type and device (``out`` may be D itself).
+    Returns (normalised points, per-dimension minima, maxima)."""
+    L = _lib.load()
+    ptr, n, d, keep, dev, stream = _prepare(D)
+    if out is None:
+        if isinstance(D, np.ndarray):
+            out = np.empty((n, d), np.float32)
+        else:
+            out = _torch().empty((n, d), dtype=_torch().float32, device=D.device)
+    optr = _out_ptr(out, n * d, np.float32, "out")
+    lo = np.empty(d, np.float32)
+    hi = np.empty(d, np.float32)
+    with _DeviceGuard(dev):
+        check(L.egg_minmax_normalize(C.c_void_p(ptr), n, d, C.c_void_p(optr), C.c_void_p(lo.ctypes.data),
+                                     C.c_void_p(hi.ctypes.data), C.c_void_p(stream) if stream else None))
+    del keep
+    return out, lo, hi
+
+
 class _Impl:
     """Stand-in for the reference's JIT module object ``impl``."""
 
@@ -266,6 +315,17 @@ class _Impl:
     def EGG_SynC_wrapper(D, eps, lam=DEFAULT_LAMBDA):
         torch = _torch()
         lab, info = egg_sync(D, eps, lam)
+        C_ = torch.from_numpy(lab.astype(np.float32))
+        itr_times = torch.tensor([t / 1000.0 for t in info["itr_ms"]], dtype=torch.float32)
+        stage_times = torch.tensor([t / 1000.0 for t in info["stage_ms"]], dtype=torch.float32)
+        space = torch.tensor([min(info["workspace_bytes"], 2**31 - 1)], dtype=torch.int32)
+        return [C_, itr_times, stage_times, space]
+
+
+    @staticmethod
+    def GPU_DynamicalClustering_wrapper(D, eps, lam=DEFAULT_LAMBDA):
+        torch = _torch()
+        lab, info = simple_sync(D, eps, lam)
         C_ = torch.from_numpy(lab.astype(np.float32))
         itr_times = torch.tensor([t / 1000.0 for t in info["itr_ms"]], dtype=torch.float32)
         stage_times = torch.tensor([t / 1000.0 for t in info["stage_ms"]], dtype=torch.float32)
@@ -281,4 +341,10 @@ def EGG_SynC(D, eps, lam=DEFAULT_LAMBDA):
     return impl.EGG_SynC_wrapper(D, eps, lam)
 
 
-__all__ = ["EGG_SynC", "impl", "egg_sync", "egg_sync_batch", "egg_step", "egg_grid", "EggError", "DEFAULT_LAMBDA"]
+def GPU_DynamicalClustering(D, eps, lam=DEFAULT_LAMBDA, call=None):
+    """python/algorithms.py:33-34: the brute-force GPU SynC."""
+    return impl.GPU_DynamicalClustering_wrapper(D, eps, lam)
+
+
+__all__ = ["EGG_SynC", "GPU_DynamicalClustering", "impl", "egg_sync", "egg_sync_batch", "egg_step", "egg_grid",
+           "normalize", "simple_sync", "EggError", "DEFAULT_LAMBDA"]

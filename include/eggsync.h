@@ -212,6 +212,28 @@ typedef struct egg_batch_stats {
 int egg_sync_batch(egg_batch_item *items, int32_t count, const egg_opts *opts, egg_batch_stats *stats,
                    void *stream);
 
+/* Brute-force SynC on the GPU, the second drop-in.  Replaces
+ * GPU_DynamicalClustering (src/algorithms/simple_GPU_SynC.cu:29-238), reached
+ * from GPU_DynamicalClustering_wrapper (src/maps/map.cpp:27-29).  Every
+ * iteration updates each point from all points within eps (itself included);
+ * the loop stops when the mean local order parameter reaches lam, or after
+ * max_iter iterations (0 = the reference's 100).  labels[n] receives, for a
+ * point whose final eps-ball holds more than one point, the rank of the
+ * smallest index in that ball, else -1.  positions_out (optional, n x d,
+ * host or device) receives the final positions.  stats (optional) receives
+ * the iteration count, converged, the number of labels, the final order
+ * parameter (order_param) and the per-iteration times (itr_ms). */
+int egg_simple_sync_run(const float *x, int64_t n, int32_t d, float eps, float lam, int32_t max_iter,
+                        int32_t *labels, float *positions_out, egg_stats *stats, void *stream);
+
+/* Per-dimension min-max normalisation of n x d float32 points on the GPU:
+ * out = (x - min) / (max - min), evaluated in float32 as python/data.py:100-103
+ * computes it on the host (0 where max == min; the reference divides by zero
+ * there).  x and out may be host or device memory and may be the same
+ * buffer.  lo and hi (optional host arrays of d floats) receive the minima
+ * and maxima.  NaN or Inf in x returns EGG_ERR_INPUT. */
+int egg_minmax_normalize(const float *x, int64_t n, int32_t d, float *out, float *lo, float *hi, void *stream);
+
 /* Learned warm start (no counterpart in the reference).  Width of one
  * feature row: feat_dim(d) = d + 3^d (1 + 2d) rounded up to a multiple of
  * 16 (192 for d = 3); -1 for d outside 1..3. */

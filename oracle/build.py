@@ -76,7 +76,8 @@ def ref_available() -> bool:
 
 
 def build_ref(force: bool = False, with_gpu: bool = True) -> dict:
-    """Compile the reference CPU SynC (and, with ``with_gpu``, EGG-SynC)."""
+    """Compile the reference CPU SynC (and, with ``with_gpu``, EGG-SynC and the
+    brute-force GPU SynC)."""
     if not ref_available():
         raise FileNotFoundError("reference sources not found under %s" % REF_ROOT)
     REF_DIR.mkdir(exist_ok=True)
@@ -116,6 +117,25 @@ def build_ref(force: bool = False, with_gpu: bool = True) -> dict:
                  ["-Xlinker", "-rpath," + link[0][2:]] + [x for x in link if not x.startswith("-Wl")] + ["-lcudart"])
             os.replace(tmp, egg_so)
         out["egg"] = egg_so
+        simple_so = REF_DIR / "libref_simple.so"
+        if force or not simple_so.exists():
+            objs = []
+            cu = [src / "algorithms" / "simple_GPU_SynC.cu", src / "utils" / "GPU_utils.cu",
+                  HERE / "ref_simple_driver.cu"]
+            for f in cu:
+                o = REF_DIR / (f.stem + ".simple.o")
+                _run(["nvcc", "-O3", "-std=c++17", "-w", "-Xcompiler", "-fPIC", abi] + ARCH +
+                     ["-I", str(src / "algorithms"), "-I", str(src / "utils")] + inc + ["-c", str(f), "-o", str(o)])
+                objs.append(str(o))
+            o = REF_DIR / "CPU_math.simple.o"
+            _run(["g++", "-O3", "-fPIC", "-std=c++17", "-w", "-include", "cstdio", abi] + inc +
+                 ["-c", str(src / "utils" / "CPU_math.cpp"), "-o", str(o)])
+            objs.append(str(o))
+            tmp = simple_so.with_suffix(".so.tmp")
+            _run(["nvcc", "-shared", "-Xcompiler", "-fPIC", "-o", str(tmp)] + objs +
+                 ["-Xlinker", "-rpath," + link[0][2:]] + [x for x in link if not x.startswith("-Wl")] + ["-lcudart"])
+            os.replace(tmp, simple_so)
+        out["simple"] = simple_so
     return out
 
 

@@ -268,6 +268,47 @@ def run_ref_egg(X, eps, timeout=600, workdir=None):
         return np.load(lout), info["iters"], info["stage_times"]
 
 
+_REF_SIMPLE_CHILD = r"""
+import sys, json, ctypes as C, numpy as np, torch
+X = np.load(sys.argv[2]).astype(np.float32)
+eps, lam = float(sys.argv[3]), float(sys.argv[4])
+L = C.CDLL(sys.argv[1])
+n, d = X.shape
+lab = np.empty(n, np.int32)
+it = C.c_int(0)
+f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+L.ref_simple_run.argtypes = [f32p, C.c_int, C.c_int, C.c_float, C.c_float, i32p, C.POINTER(C.c_int)]
+rc = L.ref_simple_run(np.ascontiguousarray(X), n, d, eps, lam, lab, C.byref(it))
+np.save(sys.argv[5], lab)
+sys.stderr.write("REF_SIMPLE_RESULT " + json.dumps({"rc": rc, "iters": it.value}) + "\n")
+"""
+
+
+def run_ref_simple(X, eps, lam=1 - 1e-3, timeout=600, workdir=None):
+    """Run the reference brute-force GPU SynC (simple_GPU_SynC.cu) on X in a
+    child process.  Returns (labels, iterations)."""
+    import tempfile
+
+    X = _as_x(X)
+    so = _build.REF_DIR / "libref_simple.so"
+    if not so.exists():
+        raise FileNotFoundError(str(so))
+    with tempfile.TemporaryDirectory(dir=workdir) as td:
+        xin = os.path.join(td, "x.npy")
+        lout = os.path.join(td, "lab.npy")
+        np.save(xin, X)
+        r = subprocess.run([sys.executable, "-c", _REF_SIMPLE_CHILD, str(so), xin, repr(float(eps)),
+                            repr(float(lam)), lout], capture_output=True, text=True, timeout=timeout)
+        info = None
+        for line in r.stderr.splitlines():
+            if line.startswith("REF_SIMPLE_RESULT "):
+                info = json.loads(line[len("REF_SIMPLE_RESULT "):])
+        if r.returncode != 0 or info is None or info["rc"] != 0:
+            raise RuntimeError("reference GPU SynC failed (rc=%s): %s" % (r.returncode, r.stderr[-2000:]))
+        return np.load(lout), info["iters"]
+
+
 def ari(a, b):
     """Adjusted Rand index with every -1 (noise) mapped to its own singleton."""
     a = np.asarray(a).astype(np.int64).copy()

@@ -12,6 +12,9 @@ oracle/build.py (oracle/_ref/):
   --gpu   reference EGG-SynC (src/algorithms/EGG_SynC.cu), needs a CUDA
           device; each case is run three times in a child process:
           ref_egg_<case>.npz labels of every run, iteration counts.
+  --gpu-simple  reference brute-force GPU SynC (src/algorithms/
+          simple_GPU_SynC.cu), needs a CUDA device; each case run twice:
+          ref_simple_<case>.npz labels of every run, iteration counts.
 
 Inputs are regenerated from their seeds by eggsync.data / the small cases
 below; each fixture stores a checksum of its input so drift is caught.
@@ -111,10 +114,36 @@ def make_gpu(out: Path, runs=3):
         print("ref_egg_%s.npz: n=%d iterations %s" % (name, len(X), its))
 
 
+def simple_cases():
+    """Inputs of the brute-force drop-in's fixtures (small: O(n^2) per iteration)."""
+    out = {}
+    for seed in (0, 1):
+        out["c1_%d" % seed] = (np.ascontiguousarray(data.c1(seed)["X"][:3000]), 0.05)
+    rng = np.random.default_rng(3)
+    out["blobs3d"] = (data.blobs(rng, 2000, 3, rng.uniform(0.2, 0.8, (4, 3)), [0.03] * 4, np.ones(4), 0.05), 0.08)
+    return out
+
+
+def make_gpu_simple(out: Path, runs=2):
+    """Labels and iteration counts of the reference's own GPU_DynamicalClustering."""
+    from oracle import run_ref_simple
+
+    for name, (X, eps) in simple_cases().items():
+        labs, its = [], []
+        for _ in range(runs):
+            lab, it = run_ref_simple(X, eps, timeout=900)
+            labs.append(lab)
+            its.append(it)
+        np.savez_compressed(out / ("ref_simple_%s.npz" % name), x_checksum=checksum(X), eps=np.float32(eps),
+                            labels=np.stack(labs), iterations=np.array(its, np.int32))
+        print("ref_simple_%s.npz: n=%d iterations %s" % (name, len(X), its))
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--cpu", action="store_true")
     ap.add_argument("--gpu", action="store_true")
+    ap.add_argument("--gpu-simple", action="store_true")
     ap.add_argument("--out", default=str(HERE))
     a = ap.parse_args()
     o = Path(a.out)
@@ -123,3 +152,5 @@ if __name__ == "__main__":
         make_cpu(o)
     if a.gpu:
         make_gpu(o)
+    if a.gpu_simple:
+        make_gpu_simple(o)

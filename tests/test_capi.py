@@ -114,6 +114,27 @@ def test_batch_argument_errors(eggsync_lib):
     assert L.egg_sync_batch(items, 2, C.byref(opts), None, None) == _lib.EGG_ERR_ARG
 
 
+def test_simple_sync_argument_errors(eggsync_lib):
+    L = eggsync_lib
+    x = np.zeros((10, 2), np.float32)
+    lab = np.zeros(10, np.int32)
+    xp, lp = C.c_void_p(x.ctypes.data), C.c_void_p(lab.ctypes.data)
+    assert L.egg_simple_sync_run(None, 10, 2, 0.05, 0.999, 0, lp, None, None, None) == _lib.EGG_ERR_ARG
+    assert L.egg_simple_sync_run(xp, 10, 2, 0.05, 0.999, 0, None, None, None, None) == _lib.EGG_ERR_ARG
+    assert L.egg_simple_sync_run(xp, 0, 2, 0.05, 0.999, 0, lp, None, None, None) == _lib.EGG_ERR_ARG
+    assert L.egg_simple_sync_run(xp, 10, 2, -1.0, 0.999, 0, lp, None, None, None) == _lib.EGG_ERR_ARG
+    assert L.egg_simple_sync_run(xp, 10, 2, 0.05, 0.999, -1, lp, None, None, None) == _lib.EGG_ERR_ARG
+
+
+def test_normalize_argument_errors(eggsync_lib):
+    L = eggsync_lib
+    x = np.zeros((10, 2), np.float32)
+    xp = C.c_void_p(x.ctypes.data)
+    assert L.egg_minmax_normalize(None, 10, 2, xp, None, None, None) == _lib.EGG_ERR_ARG
+    assert L.egg_minmax_normalize(xp, 0, 2, xp, None, None, None) == _lib.EGG_ERR_ARG
+    assert L.egg_minmax_normalize(xp, 10, 65, xp, None, None, None) == _lib.EGG_ERR_ARG
+
+
 def test_python_front_end_rejects_bad_input(eggsync_lib):
     from eggsync import egg_sync
 
