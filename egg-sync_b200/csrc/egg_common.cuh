@@ -114,6 +114,7 @@ struct Work {
     unsigned char* dirty[2];   // [n_outer]
     unsigned char* need;       // [n_outer]
     unsigned char* viol_orig;  // [ns] by original index
+    unsigned char* warp_moved; // [ns/32 + 1] the warp's points changed in the last update (grid check)
     int* span_list;            // [ns/32 + 1] cells whose points span 2-3 warps
     int* big_list;             // [ns/128 + 1] cells whose points span 4 or more warps
     // local order parameter (FP64): per-block partials, per-iteration [lo, hi]

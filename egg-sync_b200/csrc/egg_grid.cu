@@ -125,11 +125,17 @@ __device__ __forceinline__ void check_cells_body(const Geom& g, const Work& w, i
     bool changed = false;
     for (int i = bx * blockDim.x + threadIdx.x; i < g.n; i += gx * blockDim.x) {
         const int c = valid ? w.cell_of[i] : 0;
+        bool moved = false;
         for (int l = 0; l < d; l++) {
             const float x = w.Xn[(size_t)l * g.ns + i];
+            moved |= __float_as_uint(x) != __float_as_uint(w.X[(size_t)l * g.ns + i]);
             w.X[(size_t)l * g.ns + i] = x;
             if (valid) changed |= cell_dim(x, g) != w.cell_dims[(size_t)l * g.ns + c];
         }
+        // per warp of sorted points: did any of them move?  (lane 0 of the
+        // warp is active whenever any lane is: the warp's first index is < n)
+        const unsigned m = __ballot_sync(__activemask(), moved);
+        if ((threadIdx.x & 31) == 0 && w.warp_moved) w.warp_moved[i >> 5] = m != 0;
     }
     if (!valid) changed = true;
     // the incremental update's need marks are rebuilt after every grid check
@@ -137,11 +143,7 @@ __device__ __forceinline__ void check_cells_body(const Geom& g, const Work& w, i
     if (__syncthreads_or(changed) && threadIdx.x == 0) w.ctrl[kCtrlChanged] = 1;
 }
 
-__device__ __forceinline__ void build_begin_body(const Work& w) {
-    w.ctrl[kCtrlChanged] = 0;
-    w.ctrl[kCtrlSpanCount] = 0;
-    w.ctrl[kCtrlBigCount] = 0;
-}
+__device__ __forceinline__ void build_begin_body(const Work& w) { w.ctrl[kCtrlChanged] = 0; }
 
 // radix sort pass: tile histograms
 __device__ __forceinline__ void radix_hist_body(const Geom& g, const Work& w, int in_sel, int first, int dim, int shift, int bx) {
@@ -300,6 +302,9 @@ __device__ __forceinline__ void scan_block_sums_body(const Geom& g, const Work& 
         w.ctrl[kCtrlM] = total;
         w.ctrl[kCtrlGridValid] = 1;
         w.ctrl[kCtrlBuilds] += 1;
+        // the spanning-cell lists describe the grid: rebuilt with it
+        w.ctrl[kCtrlSpanCount] = 0;
+        w.ctrl[kCtrlBigCount] = 0;
     }
 }
 
@@ -354,6 +359,12 @@ __device__ __forceinline__ void cell_sums_body(const Geom& g, const Work& w, int
     const int warp = i >> 5;
     const int nw = (g.n + 31) >> 5;
     if ((i & ~31) >= g.n) return;  // whole warp beyond n
+    // Unchanged grid and none of the warp's points moved: every output of
+    // this warp (point offsets, complete-cell sums, warp partials of
+    // spanning cells) is what the last launch wrote.  The spanning-cell
+    // lists are kept from the last rebuild.
+    const bool rebuilt = w.ctrl[kCtrlChanged] != 0;
+    if (!rebuilt && w.warp_moved[i >> 5] == 0) return;
     const bool valid = i < g.n;
     const int c = valid ? w.cell_of[i] : 0x7fffffff - lane;
     const int cnext = __shfl_down_sync(0xffffffffu, c, 1);
@@ -367,7 +378,7 @@ __device__ __forceinline__ void cell_sums_body(const Geom& g, const Work& w, int
     const bool complete = seg_end && cs >= wb && ce <= wb + 32;
     // a cell that starts in this warp and continues past it: list it once
     // for the FP64 combination of its warp partials
-    if (seg_end && cs >= wb && ce > wb + 32) {
+    if (rebuilt && seg_end && cs >= wb && ce > wb + 32) {
         if (((ce - 1) >> 5) - (cs >> 5) > 2) w.big_list[atomicAdd(w.ctrl + kCtrlBigCount, 1)] = c;
         else w.span_list[atomicAdd(w.ctrl + kCtrlSpanCount, 1)] = c;
     }

@@ -183,6 +183,7 @@ size_t layout_work(const Geom& g, int max_iter, char* base, Work& w, float** xin
     add((void**)&w.dirty[1], (size_t)g.n_outer + 1);
     add((void**)&w.need, (size_t)g.n_outer + 1);
     add((void**)&w.viol_orig, ns);
+    add((void**)&w.warp_moved, (size_t)nw + 1);
     add((void**)&w.span_list, 4 * ((size_t)nw + 1));
     add((void**)&w.big_list, 4 * ((size_t)nw / 4 + 1));
     add((void**)&w.rpart, 8 * 2 * (size_t)((g.n + 127) / 128));
