@@ -538,16 +538,29 @@ __device__ __forceinline__ void cell_sums_fix_body(const Geom& g, const Work& w,
     const int d = D > 0 ? D : g.d;
     const int lane = threadIdx.x & 31;
     const int nw = (g.n + 31) >> 5;
+    // with the grid unchanged, a cell none of whose warps moved keeps its sums
+    const bool rebuilt = w.ctrl[kCtrlChanged] != 0;
     const int big = w.ctrl[kCtrlBigCount];
     const int warps = (gx * blockDim.x) >> 5;
     for (int e = (bx * blockDim.x + threadIdx.x) >> 5; e < big; e += warps) {
         const int c = w.big_list[e];
-        combine_big<D>(g, w, c, w.cell_start[c] >> 5, (w.cell_start[c + 1] - 1) >> 5, lane, nw);
+        const int wh = w.cell_start[c] >> 5, wt = (w.cell_start[c + 1] - 1) >> 5;
+        if (!rebuilt) {
+            bool any = false;
+            for (int k = wh + lane; k <= wt; k += 32) any |= w.warp_moved[k] != 0;
+            if (!__any_sync(0xffffffffu, any)) continue;
+        }
+        combine_big<D>(g, w, c, wh, wt, lane, nw);
     }
     const int count = w.ctrl[kCtrlSpanCount];
     for (int e = bx * blockDim.x + threadIdx.x; e < count; e += gx * blockDim.x) {
         const int c = w.span_list[e];
         const int wh = w.cell_start[c] >> 5, wt = (w.cell_start[c + 1] - 1) >> 5;
+        if (!rebuilt) {
+            bool any = false;
+            for (int k = wh; k <= wt; k++) any |= w.warp_moved[k] != 0;
+            if (!any) continue;
+        }
         for (int l = 0; l < d; l++) {
             double S = 0.0, Mm = 0.0, mn = 1e300, mx = -1e300;
             for (int k = wh; k <= wt; k++) {
