@@ -737,9 +737,17 @@ __global__ void k_unsort_int(Geom g, Work w, const int* __restrict__ src, int* _
         }                                                                                            \
     } while (0)
 
-void launch_build(const Exec& ex, cudaStream_t st) {
+void launch_build_check(const Exec& ex, cudaStream_t st) {
     EGG_GO(ex, kShapeOne, 32, st, build_begin);
     EGG_GO_D(ex, kShapeCapN256, 256, st, check_cells);
+}
+
+void launch_build(const Exec& ex, cudaStream_t st) {
+    launch_build_check(ex, st);
+    launch_build_sort(ex, st);
+}
+
+void launch_build_sort(const Exec& ex, cudaStream_t st) {
     if (ex.batch()) {
         for (int p = 0; p < ex.bt->max_passes; p++) {
             kb_radix_hist<<<ex.blocks(kShapeTiles, kSortThreads), kSortThreads, 0, st>>>(ex.args(kShapeTiles), p);

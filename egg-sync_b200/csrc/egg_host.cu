@@ -359,14 +359,23 @@ __global__ void k_mark_extra(Work w) {
 
 // One iteration of the loop body.  With prof (8 events), the four kernel
 // groups are bracketed by CUDA events on the launching stream.
-void enqueue_iteration(Instance& I, cudaGraphConditionalHandle h, int in_graph, cudaEvent_t* prof = nullptr) {
+// Parts of one iteration: 0 = begin + grid check, 1 = grid sort (skippable
+// when no point changed cell), 2 = the rest.
+void enqueue_part(Instance& I, int part, cudaGraphConditionalHandle h, int in_graph, cudaEvent_t* prof = nullptr) {
     cudaStream_t st = I.st;
     auto mark = [&](int k) {
         if (prof) EGG_CHECK(cudaEventRecord(prof[k], st));
     };
-    k_iter_begin<<<1, 1, 0, st>>>(I.w);
-    mark(0);
-    launch_build(single(I.g, I.w), st);
+    if (part == 0) {
+        k_iter_begin<<<1, 1, 0, st>>>(I.w);
+        mark(0);
+        launch_build_check(single(I.g, I.w), st);
+        return;
+    }
+    if (part == 1) {
+        launch_build_sort(single(I.g, I.w), st);
+        return;
+    }
     mark(1);
     mark(2);
     launch_cell_sums(single(I.g, I.w), st);
@@ -381,6 +390,15 @@ void enqueue_iteration(Instance& I, cudaGraphConditionalHandle h, int in_graph, 
     launch_extra_check(single(I.g, I.w), st);
     mark(7);
     k_iter_end<<<1, 1, 0, st>>>(I.w, h, in_graph, I.g.stop_rule);
+}
+
+void enqueue_iteration(Instance& I, cudaGraphConditionalHandle h, int in_graph, cudaEvent_t* prof = nullptr) {
+    for (int part = 0; part < 3; part++) enqueue_part(I, part, h, in_graph, prof);
+}
+
+// opens the grid-sort node of the loop graph when some point changed cell
+__global__ void k_gate_sort(Work w, cudaGraphConditionalHandle hs) {
+    cudaGraphSetConditional(hs, w.ctrl[kCtrlChanged] != 0 ? 1u : 0u);
 }
 
 std::vector<char> graph_key(const Instance& I) {
@@ -409,9 +427,42 @@ bool ensure_graph(Instance& I) {
         e = cudaGraphAddNode(&node, graph, nullptr, 0, &p);
         if (e == cudaSuccess) body = p.conditional.phGraph_out[0];
     }
+    // body: [begin, grid check, gate] -> IF(changed) [grid sort] -> [rest of the iteration]
+    cudaGraphConditionalHandle hs;
+    cudaGraphNode_t tail = nullptr, ifnode = nullptr;
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hs, body, 1, 0);
     if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(I.st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        enqueue_iteration(I, h, 1);
+        enqueue_part(I, 0, h, 1);
+        k_gate_sort<<<1, 1, 0, I.st>>>(I.w, hs);
+        cudaStreamCaptureStatus cs;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        e = cudaStreamGetCaptureInfo(I.st, &cs, nullptr, nullptr, &deps, &nd);
+        if (e == cudaSuccess && nd == 1) tail = deps[0];
+        cudaGraph_t captured = nullptr;
+        const cudaError_t e2 = cudaStreamEndCapture(I.st, &captured);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess && !tail) e = cudaErrorUnknown;
+    }
+    if (e == cudaSuccess) {
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+        cp.conditional.handle = hs;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        e = cudaGraphAddNode(&ifnode, body, &tail, 1, &cp);
+        if (e == cudaSuccess)
+            e = cudaStreamBeginCaptureToGraph(I.st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            enqueue_part(I, 1, h, 1);
+            cudaGraph_t captured = nullptr;
+            e = cudaStreamEndCapture(I.st, &captured);
+        }
+    }
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(I.st, body, &ifnode, nullptr, 1, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        enqueue_part(I, 2, h, 1);
         cudaGraph_t captured = nullptr;
         e = cudaStreamEndCapture(I.st, &captured);
     }
@@ -596,17 +647,24 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
             stats->kernel_ms[k] = kms[k];
             stats->kernel_launches[k] = kl[k];
         }
-        // launches: reset + transpose, per iteration (begin, build, 2 cell
-        // sums, update, mark, 2 extra, end), final build + labels
-        // reset + transpose; per iteration: begin, build, 2 cell sums, need,
-        // [2 order parameter], update, mark, 3 extra check, end; then the
-        // final build, labels (1 or 4 kernels), [2 cell sums + 2 order
-        // parameter], [positions]
-        const int build_l = 3 * plan_count(g) + 6;
+        // launches: reset + transpose; per iteration: begin, grid check (2),
+        // grid sort (3 per radix pass + 4), 2 cell sums, need, [2 order
+        // parameter], update, mark, 3 extra check, end; then the final
+        // build, labels (1 or 4 kernels), [2 cell sums + 2 order parameter],
+        // [positions].  In the loop graph a gate kernel runs every iteration
+        // and the grid sort only in iterations where some point changed cell.
+        const int sort_l = 3 * plan_count(g) + 4;
+        const int build_l = sort_l + 2;
         const int per_iter = build_l + 10 + ((g.order_mode == 2 || g.stop_rule == 1) ? 2 : 0);
         const int final_l = build_l + (opts.labels_mode == 1 ? 1 : 4) + (g.order_mode == 1 ? 4 : 0) +
                             (opts.positions_out ? 1 : 0);
-        stats->launches = 2 + iters * per_iter + final_l + (opts.warm_start ? 10 : 0);
+        long long loop_l = (long long)iters * per_iter;
+        if (use_graph) {
+            // grid builds in the loop: all builds but the final one when it rebuilt
+            const int loop_builds = I.h_ctrl[kCtrlBuilds] - (I.h_ctrl[kCtrlChanged] ? 1 : 0);
+            loop_l = (long long)iters * (per_iter - sort_l + 1) + (long long)loop_builds * sort_l;
+        }
+        stats->launches = (int32_t)(2 + loop_l + final_l + (opts.warm_start ? 10 : 0));
         stats->warm_started = opts.warm_start ? 1 : 0;
         stats->warm_fallback = 0;
         stats->warm_same = 0;
