@@ -59,6 +59,8 @@ struct Geom {
     int stop_rule;     // 0 = the reference's convergence flag, 1 = order parameter >= lam
     int order_mode;    // 0 = no order parameter, 1 = final only, 2 = every iteration
     float lam;         // order-parameter threshold of stop rule 1
+    int zblk;          // incremental update: cells of dimension od per block (1 block when od == d)
+    int nzb;           // ... number of blocks (<= 64: one bit each)
     int wpow[32];      // width^l for l < od
 };
 
@@ -108,11 +110,12 @@ struct Work {
     int* labels;       // [ns] output labels (original order)
     int* iter_flags;   // [max_iter] flag after each iteration
     unsigned long long* ustats;  // [kUStats] interaction counters of the update kernel (stats build)
-    // incremental update: outer cells touched by a moved point (old or new
-    // position) in the last update, ping-pong by iteration parity; the
-    // stencil dilation of those marks; the last violation bit of every point
-    unsigned char* dirty[2];   // [n_outer]
-    unsigned char* need;       // [n_outer]
+    // incremental update, per outer cell a bit mask over blocks of cells of
+    // dimension od: the blocks holding a moved point (old or new position) in
+    // the last update, ping-pong by iteration parity; their dilation over
+    // the update's candidate region; the last violation bit of every point
+    unsigned long long* dirty[2];  // [n_outer]
+    unsigned long long* need;      // [n_outer]
     unsigned char* viol_orig;  // [ns] by original index
     unsigned char* warp_moved; // [ns/32 + 1] the warp's points changed in the last update (grid check)
     int* span_list;            // [ns/32 + 1] cells whose points span 2-3 warps

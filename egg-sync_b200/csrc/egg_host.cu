@@ -91,6 +91,13 @@ Geom make_geom(int64_t n64, int d, float eps) {
     g.t_extra = sq_threshold(g.eps_extra);
     g.table_k = std::max(g.r, std::max(g.r_extra, g.r_half)) + 2;
     if (g.table_k > kMaxTable) throw ArgError{EGG_ERR_GEOMETRY, "stencil radius too large"};
+    if (od < d) {
+        g.zblk = std::max(1, (g.width + 63) / 64);
+        g.nzb = (g.width + g.zblk - 1) / g.zblk;
+    } else {
+        g.zblk = g.width;
+        g.nzb = 1;
+    }
     g.sub_dims = std::min(d, 8);
     g.sub_bits = std::max(1, 8 / g.sub_dims);
     return g;
@@ -179,9 +186,9 @@ size_t layout_work(const Geom& g, int max_iter, char* base, Work& w, float** xin
     add((void**)&w.ustats, 8 * kUStats);
     add((void**)&w.stamps, 8 * 4 * ((size_t)max_iter + 2));
     add((void**)&w.iter_flags, 4 * ((size_t)max_iter + 2));
-    add((void**)&w.dirty[0], (size_t)g.n_outer + 1);
-    add((void**)&w.dirty[1], (size_t)g.n_outer + 1);
-    add((void**)&w.need, (size_t)g.n_outer + 1);
+    add((void**)&w.dirty[0], 8 * ((size_t)g.n_outer + 1));
+    add((void**)&w.dirty[1], 8 * ((size_t)g.n_outer + 1));
+    add((void**)&w.need, 8 * ((size_t)g.n_outer + 1));
     add((void**)&w.viol_orig, ns);
     add((void**)&w.warp_moved, (size_t)nw + 1);
     add((void**)&w.span_list, 4 * ((size_t)nw + 1));
@@ -487,8 +494,8 @@ void load_input(Instance& I, const float* x, int full_update = 0) {
         src = I.xin;
     }
     k_ctrl_reset<<<1, 32, 0, I.st>>>(I.w, I.max_iter, full_update);
-    EGG_CHECK(cudaMemsetAsync(I.w.dirty[0], 0, (size_t)g.n_outer + 1, I.st));
-    EGG_CHECK(cudaMemsetAsync(I.w.dirty[1], 0, (size_t)g.n_outer + 1, I.st));
+    EGG_CHECK(cudaMemsetAsync(I.w.dirty[0], 0, 8 * ((size_t)g.n_outer + 1), I.st));
+    EGG_CHECK(cudaMemsetAsync(I.w.dirty[1], 0, 8 * ((size_t)g.n_outer + 1), I.st));
     launch_transpose_in(g, I.w, src, I.st);
 }
 
@@ -890,7 +897,7 @@ int grid_noalloc(const float* x, int64_t n, int32_t d, float eps, int32_t* order
     take((void**)&w.digit_total, 4 * 256);
     take((void**)&w.block_sums, 4 * (size_t)nb);
     take((void**)&w.ctrl, 4 * kCtrlWords);
-    take((void**)&w.need, (size_t)g.n_outer + 1);
+    take((void**)&w.need, 8 * ((size_t)g.n_outer + 1));
     take((void**)&xin, 4 * (size_t)g.n * d);
     if (off > kNoAllocBytes) throw ArgError{EGG_ERR_INTERNAL, "static scratch too small for this geometry"};
 

@@ -293,7 +293,8 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
     // or new position) anywhere in its stencil region since the last update,
     // every input of its update is unchanged, so the result is the same bit
     // for bit: keep the position and the last violation bit.
-    const bool need_me = w.ctrl[kCtrlForce] != 0 || w.need[obase] != 0;
+    const int zb = g.od < d ? gi[g.od] / g.zblk : 0;
+    const bool need_me = w.ctrl[kCtrlForce] != 0 || ((w.need[obase] >> zb) & 1ull) != 0;
     if (!__any_sync(0xffffffffu, need_me)) {
         bool viol = false;
         if (valid) {
@@ -349,7 +350,7 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
     const int N = a.N;
     const float fN = (float)N;
     bool moved = false;
-    int onew = 0;
+    int onew = 0, zbnew = 0;
     if (valid) {
         for (int l = 0; l < d; l++) {
             const float corner = __fmul_rn((float)gi[l], g.side);
@@ -361,6 +362,7 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
             w.Xn[(size_t)l * g.ns + i] = xn;
             moved |= __float_as_uint(xn) != __float_as_uint(x[l]);
             if (l < g.od) onew += cell_dim(xn, g) * g.wpow[l];
+            if (l == g.od) zbnew = cell_dim(xn, g) / g.zblk;
         }
         if (counts) counts[i] = N;
     }
@@ -378,9 +380,9 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
         }
         w.viol_orig[w.orig[i]] = viol ? 1 : 0;
         if (moved) {
-            unsigned char* dcur = w.dirty[it & 1];
-            dcur[obase] = 1;
-            dcur[onew] = 1;
+            unsigned long long* dcur = w.dirty[it & 1];
+            atomicOr(dcur + obase, 1ull << zb);
+            atomicOr(dcur + onew, 1ull << zbnew);
         }
     }
     if (__any_sync(0xffffffffu, viol) && lane == 0) {
@@ -427,17 +429,29 @@ __global__ void __launch_bounds__(T) kb_update(BatchArgs B) {
         default: KERNEL<0> __VA_ARGS__; break;        \
     }
 
-// need[] (zeroed by the grid-build check of this iteration) is set over the
-// stencil of every outer cell that the previous update marked dirty (a moved
-// point's old or new position); the marks are cleared as they are consumed,
-// so the array is clean again when the update after next writes it.
+// need[] (zeroed by the grid-build check of this iteration) receives, over
+// the stencil of every outer cell that the previous update marked dirty, the
+// dirty blocks of dimension od widened by r + 1 cells on each side: exactly
+// the points whose candidate cells (outer stencil, dimension od within
+// r + 1 cells, for_candidates) can hold a moved point's old or new position.
+// The dirty marks are cleared as they are consumed, so the array is clean
+// again when the update after next writes it.
 __device__ __forceinline__ void need_body(const Geom& g, const Work& w, int bx, int gx) {
     const int it = w.ctrl[kCtrlIter];
-    unsigned char* prev = w.dirty[(it + 1) & 1];
+    unsigned long long* prev = w.dirty[(it + 1) & 1];
     const int nst = w.st_count[0];
     for (int o = bx * blockDim.x + threadIdx.x; o < g.n_outer; o += gx * blockDim.x) {
-        if (!prev[o]) continue;
+        unsigned long long m = prev[o];
+        if (!m) continue;
         prev[o] = 0;
+        unsigned long long dil = 0;
+        while (m) {
+            const int b = __ffsll((long long)m) - 1;
+            m &= m - 1;
+            const int lo = max(0, b * g.zblk - g.r - 1);
+            const int hi = min(g.width - 1, (b + 1) * g.zblk - 1 + g.r + 1);
+            for (int k = lo / g.zblk; k <= hi / g.zblk; k++) dil |= 1ull << k;
+        }
         int co[32];
         int rem = o;
         for (int l = 0; l < g.od; l++) {
@@ -450,7 +464,7 @@ __device__ __forceinline__ void need_body(const Geom& g, const Work& w, int bx, 
                 const int v = co[l] + __ldg(w.st_off + (size_t)s * g.od + l);
                 inb = inb && (unsigned)v < (unsigned)g.width;
             }
-            if (inb) w.need[o + __ldg(w.st_delta + s)] = 1;
+            if (inb) atomicOr(w.need + o + __ldg(w.st_delta + s), dil);
         }
     }
 }
