@@ -86,6 +86,7 @@ struct Work {
     // cells (index < M, M only known on the device)
     int* cell_start;   // [ns+1]
     int* cell_dims;    // [d][ns]
+    unsigned long long* cell_key;  // [ns] the cell's dims packed 16 bits each (d <= 4): one load per box test
     int* cell_outer;   // [ns]
     float* css;        // [d][ns] sum sin(delta) per cell
     float* csm;        // [d][ns] sum (1 - cos(delta)) per cell

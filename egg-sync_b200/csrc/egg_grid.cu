@@ -328,12 +328,15 @@ __device__ __forceinline__ void heads_finalize_body(const Geom& g, const Work& w
         if (head) {
             w.cell_start[c] = i;
             int outer = 0;
+            unsigned long long key = 0;
             for (int l = 0; l < d; l++) {
                 int gl = cell_dim(w.X[(size_t)l * g.ns + i], g);
                 w.cell_dims[(size_t)l * g.ns + c] = gl;
                 if (l < g.od) outer += gl * g.wpow[l];
+                if (l < 4) key |= (unsigned long long)gl << (16 * l);
             }
             w.cell_outer[c] = outer;
+            if (d <= 4 && w.cell_key) w.cell_key[c] = key;
         }
         if (i == g.n - 1) w.cell_start[c + 1] = g.n;
     }

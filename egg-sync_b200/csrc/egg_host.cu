@@ -171,6 +171,7 @@ size_t layout_work(const Geom& g, int max_iter, char* base, Work& w, float** xin
     add((void**)&w.cell_of, 4 * ns);
     add((void**)&w.cell_start, 4 * (ns + 1));
     add((void**)&w.cell_dims, 4 * d * ns);
+    add((void**)&w.cell_key, d <= 4 ? 8 * ns : 0);
     add((void**)&w.cell_outer, 4 * ns);
     add((void**)&w.css, 4 * d * ns);
     add((void**)&w.csm, 4 * d * ns);

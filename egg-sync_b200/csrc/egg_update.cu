@@ -121,10 +121,21 @@ __device__ __forceinline__ void visit_cell(const Geom& g, const Work& w, int c, 
     const int d = D > 0 ? D : g.d;
     float sm2 = 0.f, lg2 = 0.f;
     int kk[DM];
-    for (int l = 0; l < d; l++) {
-        const int cd = __ldg(w.cell_dims + (size_t)l * g.ns + c);
-        box_terms(x[l], cd, g.side, sm2, lg2);
-        kk[l] = cd - gi[l];
+    if constexpr (D >= 1 && D <= 4) {
+        // the cell's dims from one packed word
+        const unsigned long long key = __ldg(w.cell_key + c);
+#pragma unroll
+        for (int l = 0; l < D; l++) {
+            const int cd = (int)((key >> (16 * l)) & 0xffffu);
+            box_terms(x[l], cd, g.side, sm2, lg2);
+            kk[l] = cd - gi[l];
+        }
+    } else {
+        for (int l = 0; l < d; l++) {
+            const int cd = __ldg(w.cell_dims + (size_t)l * g.ns + c);
+            box_terms(x[l], cd, g.side, sm2, lg2);
+            kk[l] = cd - gi[l];
+        }
     }
     EGG_STAT(a, kUsCells, 1);
     if (!(sm2 <= g.t_eps)) return;
