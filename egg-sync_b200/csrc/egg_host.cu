@@ -673,6 +673,8 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
             loop_l = (long long)iters * (per_iter - sort_l + 1) + (long long)loop_builds * sort_l;
         }
         stats->launches = (int32_t)(2 + loop_l + final_l + (opts.warm_start ? 10 : 0));
+        stats->grid_builds = I.h_ctrl[kCtrlBuilds];
+        stats->points_updated = (int64_t)(unsigned)I.h_ctrl[kCtrlComputed];
         stats->warm_started = opts.warm_start ? 1 : 0;
         stats->warm_fallback = 0;
         stats->warm_same = 0;

@@ -58,7 +58,8 @@ class EggStats(C.Structure):
                 ("kernel_ms", C.c_float * 4), ("kernel_launches", C.c_int32 * 4), ("launches", C.c_int32),
                 ("order_param_lo", C.c_double), ("order_param_hi", C.c_double),
                 ("itr_order_param", C.POINTER(C.c_double)), ("warm_started", C.c_int32),
-                ("warm_fallback", C.c_int32), ("warm_ms", C.c_float), ("warm_same", C.c_int32)]
+                ("warm_fallback", C.c_int32), ("warm_ms", C.c_float), ("warm_same", C.c_int32),
+                ("grid_builds", C.c_int32), ("points_updated", C.c_int64)]
 
 
 class EggBatchItem(C.Structure):

@@ -165,6 +165,8 @@ def egg_sync(D, eps: float, lam: float = DEFAULT_LAMBDA, max_iter: int = 0, loop
         "warm_fallback": bool(stats.warm_fallback),
         "warm_same": bool(stats.warm_same),
         "warm_ms": float(stats.warm_ms),
+        "grid_builds": int(stats.grid_builds),
+        "points_updated": int(stats.points_updated),
     }
     del mlp
     return labels_out, info

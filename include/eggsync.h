@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define EGG_SYNC_ABI_VERSION 3
+#define EGG_SYNC_ABI_VERSION 4
 
 typedef enum egg_status {
     EGG_OK = 0,
@@ -111,6 +111,9 @@ typedef struct egg_stats {
     int32_t warm_fallback; /* 1 when warm_verify found a different partition and returned the plain run */
     float warm_ms;         /* device time of the warm start (features + network + displacement) */
     int32_t warm_same;     /* warm_verify: 1 when the two partitions were identical */
+    int32_t grid_builds;   /* grid builds performed (iterations where some point changed cell, the
+                              first and the final build included) */
+    int64_t points_updated; /* point updates computed; the rest reused their previous result */
 } egg_stats;
 
 /* Fill *opts with the defaults (all zero). */

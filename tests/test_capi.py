@@ -33,7 +33,7 @@ def test_exports_every_declared_symbol(eggsync_lib):
 
 
 def test_abi_version_and_status_names(eggsync_lib):
-    assert eggsync_lib.egg_abi_version() == 3
+    assert eggsync_lib.egg_abi_version() == 4
     # the normal build collects no interaction counters
     buf = (C.c_int64 * 16)()
     assert eggsync_lib.egg_update_counters(buf, 16) == 0
@@ -47,7 +47,7 @@ def test_struct_layout_matches_header(tmp_path):
     fields = [("egg_opts", _lib.EggOpts, ["positions_out", "labels_mode", "batch_tune", "warm_start",
                                            "warm_verify"]),
               ("egg_stats", _lib.EggStats, ["stage_ms", "itr_ms", "itr_cap", "itr_order_param", "warm_ms",
-                                            "warm_same"]),
+                                            "warm_same", "grid_builds", "points_updated"]),
               ("egg_mlp", _lib.EggMlp, ["min_count", "w1", "b3"]),
               ("egg_mlp_train_opts", _lib.EggMlpTrainOpts, ["lr", "seed"]),
               ("egg_batch_item", _lib.EggBatchItem, ["n", "eps", "labels", "status"]),
