@@ -121,6 +121,7 @@ struct Work {
     unsigned char* warp_moved; // [ns/32 + 1] the warp's points changed in the last update (grid check)
     int* span_list;            // [ns/32 + 1] cells whose points span 2-3 warps
     int* big_list;             // [ns/128 + 1] cells whose points span 4 or more warps
+    int* span_mark;            // [ns] per spanning cell: the last iteration that re-summed one of its warps
     // local order parameter (FP64): per-block partials, per-iteration [lo, hi]
     double* rpart;             // [2 * blocks]
     double* rvals;             // [2 * (max_iter + 2)]; slot max_iter + 1 = final value

@@ -379,6 +379,10 @@ __device__ __forceinline__ void cell_sums_body(const Geom& g, const Work& w, int
         ce = w.cell_start[c + 1];
     }
     const bool complete = seg_end && cs >= wb && ce <= wb + 32;
+    // a spanning cell with a warp re-summed in this iteration: its warp
+    // partials are combined again (every warp holding a point of the cell
+    // has a segment end for it)
+    if (seg_end && !complete) w.span_mark[c] = w.ctrl[kCtrlIter];
     // a cell that starts in this warp and continues past it: list it once
     // for the FP64 combination of its warp partials
     if (rebuilt && seg_end && cs >= wb && ce > wb + 32) {
@@ -478,14 +482,45 @@ __device__ void combine_big(const Geom& g, const Work& w, int c, int wh, int wt,
         double S[DM], Mm[DM], mn[DM], mx[DM];
 #pragma unroll
         for (int l = 0; l < DM; l++) { S[l] = 0.0; Mm[l] = 0.0; mn[l] = 1e300; mx[l] = -1e300; }
-        for (int k = wh + lane; k <= wt; k += 32) {
-            const int rec = (k == wh) ? 1 : 0;
+        // kBatch partials per lane in flight: all their loads first, then
+        // the accumulation in the lane's order k = wh + lane, +32, ...
+        // (wide d: one at a time, the accumulators fill the registers)
+        constexpr int kBatch = DM <= 4 ? 4 : 1;
+        if constexpr (kBatch == 1) {
+            for (int k = wh + lane; k <= wt; k += 32) {
+                const int rec = (k == wh) ? 1 : 0;
 #pragma unroll
-            for (int l = 0; l < DM; l++) {
-                S[l] += w.wpart[wp_idx(0, l, d, rec, nw, k)];
-                Mm[l] += w.wpart[wp_idx(1, l, d, rec, nw, k)];
-                mn[l] = fmin(mn[l], w.wpart[wp_idx(2, l, d, rec, nw, k)]);
-                mx[l] = fmax(mx[l], w.wpart[wp_idx(3, l, d, rec, nw, k)]);
+                for (int l = 0; l < DM; l++) {
+                    S[l] += w.wpart[wp_idx(0, l, d, rec, nw, k)];
+                    Mm[l] += w.wpart[wp_idx(1, l, d, rec, nw, k)];
+                    mn[l] = fmin(mn[l], w.wpart[wp_idx(2, l, d, rec, nw, k)]);
+                    mx[l] = fmax(mx[l], w.wpart[wp_idx(3, l, d, rec, nw, k)]);
+                }
+            }
+        } else {
+            for (int k0 = wh + lane; k0 <= wt; k0 += 32 * kBatch) {
+                double v[kBatch][4][DM];
+#pragma unroll
+                for (int u = 0; u < kBatch; u++) {
+                    const int k = k0 + 32 * u;
+                    const int kk = k <= wt ? k : k0;  // in-range stand-in, not accumulated
+                    const int rec = (kk == wh) ? 1 : 0;
+#pragma unroll
+                    for (int l = 0; l < DM; l++)
+#pragma unroll
+                        for (int f = 0; f < 4; f++) v[u][f][l] = w.wpart[wp_idx(f, l, d, rec, nw, kk)];
+                }
+#pragma unroll
+                for (int u = 0; u < kBatch; u++) {
+                    if (k0 + 32 * u > wt) break;
+#pragma unroll
+                    for (int l = 0; l < DM; l++) {
+                        S[l] += v[u][0][l];
+                        Mm[l] += v[u][1][l];
+                        mn[l] = fmin(mn[l], v[u][2][l]);
+                        mx[l] = fmax(mx[l], v[u][3][l]);
+                    }
+                }
             }
         }
 #pragma unroll
@@ -542,28 +577,22 @@ __device__ __forceinline__ void cell_sums_fix_body(const Geom& g, const Work& w,
     const int lane = threadIdx.x & 31;
     const int nw = (g.n + 31) >> 5;
     // with the grid unchanged, a cell none of whose warps moved keeps its sums
+    // (marked by the cell-sums kernel of this iteration)
     const bool rebuilt = w.ctrl[kCtrlChanged] != 0;
+    const int it = w.ctrl[kCtrlIter];
     const int big = w.ctrl[kCtrlBigCount];
     const int warps = (gx * blockDim.x) >> 5;
     for (int e = (bx * blockDim.x + threadIdx.x) >> 5; e < big; e += warps) {
         const int c = w.big_list[e];
+        if (!rebuilt && w.span_mark[c] != it) continue;  // uniform across the warp
         const int wh = w.cell_start[c] >> 5, wt = (w.cell_start[c + 1] - 1) >> 5;
-        if (!rebuilt) {
-            bool any = false;
-            for (int k = wh + lane; k <= wt; k += 32) any |= w.warp_moved[k] != 0;
-            if (!__any_sync(0xffffffffu, any)) continue;
-        }
         combine_big<D>(g, w, c, wh, wt, lane, nw);
     }
     const int count = w.ctrl[kCtrlSpanCount];
     for (int e = bx * blockDim.x + threadIdx.x; e < count; e += gx * blockDim.x) {
         const int c = w.span_list[e];
+        if (!rebuilt && w.span_mark[c] != it) continue;
         const int wh = w.cell_start[c] >> 5, wt = (w.cell_start[c + 1] - 1) >> 5;
-        if (!rebuilt) {
-            bool any = false;
-            for (int k = wh; k <= wt; k++) any |= w.warp_moved[k] != 0;
-            if (!any) continue;
-        }
         for (int l = 0; l < d; l++) {
             double S = 0.0, Mm = 0.0, mn = 1e300, mx = -1e300;
             for (int k = wh; k <= wt; k++) {

@@ -194,6 +194,7 @@ size_t layout_work(const Geom& g, int max_iter, char* base, Work& w, float** xin
     add((void**)&w.warp_moved, (size_t)nw + 1);
     add((void**)&w.span_list, 4 * ((size_t)nw + 1));
     add((void**)&w.big_list, 4 * ((size_t)nw / 4 + 1));
+    add((void**)&w.span_mark, 4 * ns);
     add((void**)&w.rpart, 8 * 2 * (size_t)((g.n + 127) / 128));
     add((void**)&w.rvals, 8 * 2 * ((size_t)max_iter + 2));
     add((void**)&w.uf_parent, 4 * ns);
