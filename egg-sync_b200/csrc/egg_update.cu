@@ -447,35 +447,47 @@ __global__ void __launch_bounds__(T) kb_update(BatchArgs B) {
 // r + 1 cells, for_candidates) can hold a moved point's old or new position.
 // The dirty marks are cleared as they are consumed, so the array is clean
 // again when the update after next writes it.
+// A warp reads 32 outer cells at once; the lanes share the stencil entries
+// of each dirty one (dirty cells cluster around the regions still moving, so
+// a thread per cell would leave a few SMs with all the atomics).
 __device__ __forceinline__ void need_body(const Geom& g, const Work& w, int bx, int gx) {
     const int it = w.ctrl[kCtrlIter];
     unsigned long long* prev = w.dirty[(it + 1) & 1];
     const int nst = w.st_count[0];
-    for (int o = bx * blockDim.x + threadIdx.x; o < g.n_outer; o += gx * blockDim.x) {
-        unsigned long long m = prev[o];
-        if (!m) continue;
-        prev[o] = 0;
-        unsigned long long dil = 0;
-        while (m) {
-            const int b = __ffsll((long long)m) - 1;
-            m &= m - 1;
-            const int lo = max(0, b * g.zblk - g.r - 1);
-            const int hi = min(g.width - 1, (b + 1) * g.zblk - 1 + g.r + 1);
-            for (int k = lo / g.zblk; k <= hi / g.zblk; k++) dil |= 1ull << k;
-        }
-        int co[32];
-        int rem = o;
-        for (int l = 0; l < g.od; l++) {
-            co[l] = rem % g.width;
-            rem /= g.width;
-        }
-        for (int s = 0; s < nst; s++) {
-            bool inb = true;
-            for (int l = 0; l < g.od; l++) {
-                const int v = co[l] + __ldg(w.st_off + (size_t)s * g.od + l);
-                inb = inb && (unsigned)v < (unsigned)g.width;
+    const int lane = threadIdx.x & 31;
+    // warp-uniform loop over chunks of 32 outer cells
+    for (int o0 = bx * blockDim.x + (threadIdx.x & ~31); o0 < g.n_outer; o0 += gx * blockDim.x) {
+        const int o = o0 + lane;
+        const unsigned long long mine = o < g.n_outer ? prev[o] : 0ull;
+        if (mine) prev[o] = 0;
+        unsigned todo = __ballot_sync(0xffffffffu, mine != 0);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            unsigned long long m = __shfl_sync(0xffffffffu, mine, src);
+            const int oc = o0 + src;
+            unsigned long long dil = 0;
+            while (m) {
+                const int b = __ffsll((long long)m) - 1;
+                m &= m - 1;
+                const int lo = max(0, b * g.zblk - g.r - 1);
+                const int hi = min(g.width - 1, (b + 1) * g.zblk - 1 + g.r + 1);
+                for (int k = lo / g.zblk; k <= hi / g.zblk; k++) dil |= 1ull << k;
             }
-            if (inb) atomicOr(w.need + o + __ldg(w.st_delta + s), dil);
+            int co[32];
+            int rem = oc;
+            for (int l = 0; l < g.od; l++) {
+                co[l] = rem % g.width;
+                rem /= g.width;
+            }
+            for (int s = lane; s < nst; s += 32) {
+                bool inb = true;
+                for (int l = 0; l < g.od; l++) {
+                    const int v = co[l] + __ldg(w.st_off + (size_t)s * g.od + l);
+                    inb = inb && (unsigned)v < (unsigned)g.width;
+                }
+                if (inb) atomicOr(w.need + oc + __ldg(w.st_delta + s), dil);
+            }
         }
     }
 }
