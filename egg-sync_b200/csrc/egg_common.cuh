@@ -93,6 +93,7 @@ struct Work {
     float* cbmin;      // [d][ns] tight bounding box of the cell's points
     float* cbmax;      // [d][ns]
     int* outer_begin;  // [n_outer + 1]
+    unsigned long long* colmask;  // [n_outer] per outer cell: the blocks of zblk cells of dimension od holding a cell
     // scratch for scans / sorts
     int* hist;         // [256 * tiles]
     int* digit_total;  // [256]

@@ -342,12 +342,23 @@ __device__ __forceinline__ void heads_finalize_body(const Geom& g, const Work& w
     }
 }
 
-// outer_begin[o] = first cell whose outer id >= o, o in [0, n_outer]
+// outer_begin[o] = first cell whose outer id >= o, o in [0, n_outer]; with
+// od < d, colmask[o] = the blocks of dimension od (zblk cells each, bit
+// z / zblk) that hold a cell of outer cell o
 __device__ __forceinline__ void outer_ranges_body(const Geom& g, const Work& w, int bx, int gx) {
     EGG_SKIP_IF_UNCHANGED(w.ctrl);
     const int M = w.ctrl[kCtrlM];
-    for (int o = bx * blockDim.x + threadIdx.x; o <= g.n_outer; o += gx * blockDim.x)
-        w.outer_begin[o] = lower_bound_i(w.cell_outer, 0, M, o);
+    const bool cols = g.od < g.d && w.colmask != nullptr;
+    const int* z = w.cell_dims + (size_t)g.od * g.ns;
+    for (int o = bx * blockDim.x + threadIdx.x; o <= g.n_outer; o += gx * blockDim.x) {
+        const int b = lower_bound_i(w.cell_outer, 0, M, o);
+        w.outer_begin[o] = b;
+        if (cols && o < g.n_outer) {
+            unsigned long long m = 0;
+            for (int c = b; c < M && w.cell_outer[c] == o; c++) m |= 1ull << (z[c] / g.zblk);
+            w.colmask[o] = m;
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------

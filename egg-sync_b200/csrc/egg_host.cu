@@ -178,6 +178,7 @@ size_t layout_work(const Geom& g, int max_iter, char* base, Work& w, float** xin
     add((void**)&w.cbmin, 4 * d * ns);
     add((void**)&w.cbmax, 4 * d * ns);
     add((void**)&w.outer_begin, 4 * ((size_t)g.n_outer + 1));
+    add((void**)&w.colmask, g.od < d ? 8 * ((size_t)g.n_outer + 1) : 0);
     add((void**)&w.hist, 4 * 256 * (size_t)tiles);
     add((void**)&w.digit_total, 4 * 256);
     add((void**)&w.block_sums, 4 * (size_t)nb);

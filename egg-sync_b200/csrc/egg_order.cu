@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(128) k_order_param(Geom g, Work w) {
         }
         double lo = 0.0, hi = 0.0;
         int N = 0;
-        for_candidates(g, w, gi, obase, lane, d, [&](int c) { order_cell<D>(g, w, c, x, lo, hi, N); });
+        for_candidates(g, w, gi, obase, lane, d, [] { return true; }, [&](int c) { order_cell<D>(g, w, c, x, lo, hi, N); });
         if (valid && N > 0) {
             rlo = lo / (double)N;
             rhi = hi / (double)N;

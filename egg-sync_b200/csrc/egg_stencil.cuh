@@ -11,16 +11,31 @@
 // entry) and visits each candidate cell with all lanes in lockstep (the cell
 // records become broadcast loads); otherwise each lane walks its own stencil.
 // fn(c) is called once per candidate cell per lane, in increasing stencil
-// entry then increasing cell order in both paths.
+// entry then increasing cell order in both paths.  A lane for which
+// active() is false needs no result: it rides along in the lockstep path
+// and skips its own walk in the other (active() is evaluated there only, so
+// the lockstep path carries nothing extra).
+//
+// In a lane's own walk with od < d, an outer cell none of whose blocks of
+// dimension od (colmask) meets the lane's z-window holds no candidate: it is
+// passed over without the two binary searches (the same empty range they
+// would give).
+
 #pragma once
 
 #include "egg_common.cuh"
 
 namespace egg {
 
-template <typename F>
+// colmask bits of the blocks meeting the cells [zl, zh] of dimension od
+__device__ __forceinline__ unsigned long long zwindow_mask(const Geom& g, int zl, int zh) {
+    const int bl = max(0, zl) / g.zblk, bh = min(g.width - 1, zh) / g.zblk;
+    return (2ull << bh) - (1ull << bl);  // bits bl..bh (bh = 63 wraps to the right value)
+}
+
+template <typename A, typename F>
 __device__ __forceinline__ void for_candidates(const Geom& g, const Work& w, const int* gi, int obase, int lane,
-                                               int d, F&& fn) {
+                                               int d, A&& active, F&& fn) {
     const int nst = w.st_count[0];
     const int ob0 = __shfl_sync(0xffffffffu, obase, 0);
     if (__all_sync(0xffffffffu, obase == ob0)) {
@@ -63,22 +78,42 @@ __device__ __forceinline__ void for_candidates(const Geom& g, const Work& w, con
             }
         }
     } else {
-        for (int s = 0; s < nst; s++) {
-            bool inb = true;
-            for (int l = 0; l < g.od; l++) {
-                const int v = gi[l] + __ldg(w.st_off + (size_t)s * g.od + l);
-                inb = inb && (unsigned)v < (unsigned)g.width;
+        if (!active()) return;  // no warp-wide operation below
+        // each lane walks its own stencil; the column masks of four entries
+        // are loaded together, so most columns cost a quarter of a load
+        constexpr int kAhead = 4;
+        const bool zs = g.od < d && w.colmask != nullptr;
+        const unsigned long long wm = zs ? zwindow_mask(g, gi[g.od] - g.r - 1, gi[g.od] + g.r + 1) : 0ull;
+        for (int s0 = 0; s0 < nst; s0 += kAhead) {
+            int ol[kAhead];
+#pragma unroll
+            for (int k = 0; k < kAhead; k++) {
+                const int s = s0 + k;
+                ol[k] = -1;
+                if (s < nst) {
+                    bool inb = true;
+                    for (int l = 0; l < g.od; l++) {
+                        const int v = gi[l] + __ldg(w.st_off + (size_t)s * g.od + l);
+                        inb = inb && (unsigned)v < (unsigned)g.width;
+                    }
+                    const int o = obase + __ldg(w.st_delta + s);
+                    if (inb && zs) inb = (__ldg(w.colmask + o) & wm) != 0;
+                    if (inb) ol[k] = o;
+                }
             }
-            if (!inb) continue;
-            const int o = obase + __ldg(w.st_delta + s);
-            int cb = __ldg(w.outer_begin + o), ce = __ldg(w.outer_begin + o + 1);
-            if (cb >= ce) continue;
-            if (g.od < d) {
-                const int* keys = w.cell_dims + (size_t)g.od * g.ns;
-                cb = lower_bound_i(keys, cb, ce, gi[g.od] - g.r - 1);
-                ce = lower_bound_i(keys, cb, ce, gi[g.od] + g.r + 2);
+#pragma unroll 1
+            for (int k = 0; k < kAhead; k++) {
+                const int o = ol[k];
+                if (o < 0) continue;
+                int cb = __ldg(w.outer_begin + o), ce = __ldg(w.outer_begin + o + 1);
+                if (cb >= ce) continue;
+                if (g.od < d) {
+                    const int* keys = w.cell_dims + (size_t)g.od * g.ns;
+                    cb = lower_bound_i(keys, cb, ce, gi[g.od] - g.r - 1);
+                    ce = lower_bound_i(keys, cb, ce, gi[g.od] + g.r + 2);
+                }
+                for (int c = cb; c < ce; c++) fn(c);
             }
-            for (int c = cb; c < ce; c++) fn(c);
         }
     }
 }

@@ -318,8 +318,17 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
         }
         return;
     }
+    // Within a warp that recomputes, a lane whose own region is clean keeps
+    // its result too (same argument, per point): it does not walk when the
+    // lanes walk separately (lanes in several outer cells), where the walks
+    // of a warp's lanes run one after another.  The lane's need bit is read
+    // again where it is used, so nothing extra stays live over the walk.
+    auto lane_needs = [&]() {
+        return counts != nullptr || w.ctrl[kCtrlForce] != 0 ||
+               ((w.need[obase] >> (g.od < d ? gi[g.od] / g.zblk : 0)) & 1ull) != 0;
+    };
     {
-        const unsigned vm = __ballot_sync(0xffffffffu, valid);
+        const unsigned vm = __ballot_sync(0xffffffffu, valid && (need_me || counts != nullptr));
         if (lane == 0) atomicAdd(w.ctrl + kCtrlComputed, __popc(vm));
     }
 
@@ -348,7 +357,7 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
 #ifdef EGG_UPDATE_STATS
     const long long t_walk0 = clock64();
 #endif
-    for_candidates(g, w, gi, obase, lane, d,
+    for_candidates(g, w, gi, obase, lane, d, lane_needs,
                    [&](int c) { visit_cell<D>(g, w, c, x, gi, a, Ts, Tc, Tm, K, TW); });
 #ifdef EGG_UPDATE_STATS
     {
@@ -358,11 +367,14 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
     }
 #endif
 
+    const bool walk = lane_needs();
     const int N = a.N;
     const float fN = (float)N;
     bool moved = false;
     int onew = 0, zbnew = 0;
-    if (valid) {
+    if (valid && !walk) {
+        for (int l = 0; l < d; l++) w.Xn[(size_t)l * g.ns + i] = x[l];
+    } else if (valid) {
         for (int l = 0; l < d; l++) {
             const float corner = __fmul_rn((float)gi[l], g.side);
             const float phi = x[l] - corner;
@@ -381,7 +393,9 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
     // convergence flag, EGG_SynC.cu:706-709.  half_count <= N - partial_in,
     // so a border point with neighbours in a partial cell always violates.
     bool viol = false;
-    if (valid) {
+    if (valid && !walk) {
+        viol = w.viol_orig[w.orig[i]] != 0;
+    } else if (valid) {
         if (!border) viol = (N != own_cnt);
         else if (a.partial_in > 0) viol = true;
         else if (N == own_cnt) viol = false;
@@ -402,11 +416,14 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
     }
     if (a.tab_err) atomicOr(w.ctrl + kCtrlStatus, kErrTable);
 #ifdef EGG_UPDATE_STATS
-    if (valid) {
+    if (valid && walk) {
         a.st[kUsPoints] += 1;
         a.st[kUsNeighbors] += N;
     } else {
-        for (int k = 0; k < kUStats; k++) if (k != kUsLaneWarps) a.st[k] = 0;  // shadow lanes
+        // shadow lanes, and lanes that kept their result (their lockstep
+        // visits are not work of the update)
+        for (int k = 0; k < kUStats; k++)
+            if (k != kUsLaneWarps && k != kUsCyclesShared && k != kUsCyclesLane) a.st[k] = 0;
     }
     for (int k = 0; k < kUStats; k++) {
         unsigned long long v = a.st[k];
