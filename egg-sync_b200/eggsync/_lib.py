@@ -25,7 +25,8 @@ EGG_ERR_INTERNAL = -6
 EXPORTS = ("egg_opts_default", "egg_sync_run", "egg_sync_step", "egg_sync_grid", "egg_sync_grid_noalloc",
            "egg_sync_batch", "egg_status_str", "egg_last_error", "egg_release", "egg_abi_version",
            "egg_update_counters", "egg_mlp_feature_dim", "egg_mlp_features", "egg_mlp_forward", "egg_mlp_grad",
-           "egg_mlp_train", "egg_minmax_normalize", "egg_simple_sync_run")
+           "egg_mlp_train", "egg_minmax_normalize", "egg_simple_sync_run", "egg_knn_mean", "egg_mdl_cost",
+           "egg_mdl_search")
 
 # egg_update_counters slots
 UPDATE_COUNTERS = ("points", "cells", "small_pass", "full", "tight_in", "tight_out", "groups_in", "groups_out",
@@ -74,6 +75,14 @@ class EggBatchStats(C.Structure):
                 ("order", C.c_int32), ("reserved0", C.c_int32), ("workspace_bytes", C.c_int64),
                 ("total_ms", C.c_float), ("loop_ms", C.c_float), ("tune_ms", C.c_float),
                 ("itr_cap", C.c_int32), ("itr_ms", C.POINTER(C.c_float)), ("reserved", C.c_int32 * 2)]
+
+
+class EggMdlStats(C.Structure):
+    _fields_ = [("eps0", C.c_double), ("eps1", C.c_double), ("eps_step", C.c_float), ("eps_best", C.c_float),
+                ("candidates", C.c_int32), ("best", C.c_int32), ("n_clusters", C.c_int32),
+                ("end_reason", C.c_int32), ("cost_best", C.c_double), ("total_ms", C.c_float),
+                ("cap", C.c_int32), ("costs", C.POINTER(C.c_double)), ("eps", C.POINTER(C.c_float)),
+                ("clusters", C.POINTER(C.c_int32))]
 
 
 class EggError(RuntimeError):
@@ -128,6 +137,12 @@ def load():
     L.egg_simple_sync_run.argtypes = [vp, C.c_int64, C.c_int32, C.c_float, C.c_float, C.c_int32, vp, vp,
                                       C.POINTER(EggStats), vp]
     L.egg_simple_sync_run.restype = C.c_int
+    L.egg_knn_mean.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, C.POINTER(C.c_double), vp]
+    L.egg_knn_mean.restype = C.c_int
+    L.egg_mdl_cost.argtypes = [vp, C.c_int64, C.c_int32, vp, C.POINTER(C.c_double), C.POINTER(C.c_int32), vp]
+    L.egg_mdl_cost.restype = C.c_int
+    L.egg_mdl_search.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, C.c_int32, vp, C.POINTER(EggMdlStats), vp]
+    L.egg_mdl_search.restype = C.c_int
     L.egg_minmax_normalize.argtypes = [vp, C.c_int64, C.c_int32, vp, vp, vp, vp]
     L.egg_minmax_normalize.restype = C.c_int
     L.egg_mlp_feature_dim.argtypes = [C.c_int32]

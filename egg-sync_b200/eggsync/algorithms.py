@@ -310,6 +310,70 @@ def normalize(D, out=None):
     return out, lo, hi
 
 
+def knn_mean(D, k: int):
+    """Mean distance of the points to their k-th and (k+1)-th nearest other
+    point (python/SynCTorch.py:112-137, NN(k, D) and NN(k+1, D)), on the
+    GPU.  Returns (NN(k), NN(k+1))."""
+    L = _lib.load()
+    ptr, n, d, keep, dev, stream = _prepare(D)
+    out = (C.c_double * 2)()
+    with _DeviceGuard(dev):
+        check(L.egg_knn_mean(C.c_void_p(ptr), n, d, int(k), out, C.c_void_p(stream) if stream else None))
+    del keep
+    return float(out[0]), float(out[1])
+
+
+def mdl_cost(D, labels) -> Tuple[float, int]:
+    """Coding cost of the clustering given by ``labels`` (>= 0: cluster id,
+    -1: outlier), L_Clust_Outl (python/SynCTorch.py:265-314), on the GPU.
+    Returns (cost, number of clusters)."""
+    L = _lib.load()
+    ptr, n, d, keep, dev, stream = _prepare(D)
+    lab = labels
+    if isinstance(lab, np.ndarray):
+        lab = np.ascontiguousarray(lab, np.int32)
+    lptr = _out_ptr(lab, n, np.int32, "labels")
+    cost = C.c_double()
+    k = C.c_int32()
+    with _DeviceGuard(dev):
+        check(L.egg_mdl_cost(C.c_void_p(ptr), n, d, C.c_void_p(lptr), C.byref(cost), C.byref(k),
+                             C.c_void_p(stream) if stream else None))
+    del keep
+    return float(cost.value), int(k.value)
+
+
+def mdl_search(D, k: int, max_candidates: int = 0, labels_out=None):
+    """The full-SynC eps search, Sync(D, k) (python/SynCTorch.py:349-372):
+    eps from NN(k) in steps of NN(k+1) - NN(k), each eps clustered with
+    EGG-SynC and costed by L_Clust_Outl, stopping after the first clustering
+    with one cluster; returns (labels of the clustering of least cost, info)."""
+    L = _lib.load()
+    ptr, n, d, keep, dev, stream = _prepare(D)
+    if labels_out is None:
+        labels_out = np.empty(n, np.int32)
+    lptr = _out_ptr(labels_out, n, np.int32, "labels_out")
+    cap = max_candidates if max_candidates > 0 else 256
+    costs = (C.c_double * cap)()
+    epss = (C.c_float * cap)()
+    ks = (C.c_int32 * cap)()
+    st = _lib.EggMdlStats()
+    st.cap = cap
+    st.costs = C.cast(costs, C.POINTER(C.c_double))
+    st.eps = C.cast(epss, C.POINTER(C.c_float))
+    st.clusters = C.cast(ks, C.POINTER(C.c_int32))
+    with _DeviceGuard(dev):
+        check(L.egg_mdl_search(C.c_void_p(ptr), n, d, int(k), int(max_candidates), C.c_void_p(lptr), C.byref(st),
+                               C.c_void_p(stream) if stream else None))
+    del keep
+    m = min(st.candidates, cap)
+    info = {"eps0": st.eps0, "eps1": st.eps1, "eps_step": st.eps_step, "eps_best": st.eps_best,
+            "candidates": st.candidates, "best": st.best, "n_clusters": st.n_clusters,
+            "end_reason": {0: "one cluster", 1: "candidate cap", 2: "eps beyond the grid"}[st.end_reason],
+            "cost_best": st.cost_best, "total_ms": st.total_ms, "costs": [costs[i] for i in range(m)],
+            "eps": [epss[i] for i in range(m)], "clusters": [ks[i] for i in range(m)]}
+    return labels_out, info
+
+
 class _Impl:
     """Stand-in for the reference's JIT module object ``impl``."""
 

@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define EGG_SYNC_ABI_VERSION 4
+#define EGG_SYNC_ABI_VERSION 5
 
 typedef enum egg_status {
     EGG_OK = 0,
@@ -289,6 +289,58 @@ int egg_abi_version(void);
  * (libeggsync_stats.so) collects them; it writes min(cap, 16) values and
  * returns 16.  The normal build returns 0.  No counterpart in the reference. */
 int egg_update_counters(int64_t *out, int32_t cap);
+
+/* ---- eps search by minimum description length ------------------------- */
+
+/* Mean distance of the points to their k-th and (k+1)-th nearest other
+ * point, out[0] and out[1] (FP64 means of FP32 distances).  Replaces
+ * NN(k, D) (python/SynCTorch.py:112-137), which the reference calls for k
+ * and k+1.  1 <= k <= 31, n >= k + 2; x n x d float32 row-major, host or
+ * device.  Brute force on the GPU, O(n^2 d). */
+int egg_knn_mean(const float *x, int64_t n, int32_t d, int32_t k, double *out, void *stream);
+
+/* Coding cost of a clustering, L_Clust_Outl(D, M)
+ * (python/SynCTorch.py:265-314): clusters are the points sharing a label
+ * >= 0, label -1 marks an outlier (the labels egg_sync_run returns).  With
+ * h_l = 0.9 n^(-1/(d+4)) min(var_l, IQR_l / 1.34) (var the unbiased
+ * variance of dimension l, IQR its 75th minus 25th percentile) and f(x) the
+ * Gaussian product-kernel density of x among its own cluster's points:
+ *   cost = sum_C (|C| log2(n/|C|) + d/2 log2|C|) + outliers log2 n
+ *          - sum_C sum_{x in C} log2(f(x) / sum_{y in C} f(y))
+ *          - outliers (2 pi)^(-1/2) prod_l h_l.
+ * Writes *cost and (optional) *clusters.  x and labels host or device. */
+int egg_mdl_cost(const float *x, int64_t n, int32_t d, const int32_t *labels, double *cost, int32_t *clusters,
+                 void *stream);
+
+typedef struct egg_mdl_stats {
+    double eps0;          /* NN(k) */
+    double eps1;          /* NN(k+1) */
+    float eps_step;       /* float32 NN(k+1) - NN(k): the eps schedule's step */
+    float eps_best;       /* eps of the returned clustering */
+    int32_t candidates;   /* eps values clustered and costed */
+    int32_t best;         /* index of the returned candidate */
+    int32_t n_clusters;   /* clusters of the returned clustering */
+    int32_t end_reason;   /* 0: a clustering had one cluster (the reference's stop), 1: candidate cap,
+                             2: the next eps is beyond what the grid takes */
+    double cost_best;     /* its coding cost */
+    float total_ms;       /* device time of the call */
+    int32_t cap;          /* in: entries of the optional arrays below */
+    double *costs;        /* optional [cap]: cost of every candidate, in order */
+    float *eps;           /* optional [cap]: eps of every candidate */
+    int32_t *clusters;    /* optional [cap]: clusters of every candidate */
+} egg_mdl_stats;
+
+/* The full-SynC eps search, Sync(D, k) (python/SynCTorch.py:349-372):
+ * eps starts at NN(k) and grows by NN(k+1) - NN(k) (float32 arithmetic);
+ * every eps is clustered with the EGG-SynC loop (eight candidates per
+ * batched call, each identical to egg_sync_run with default options) and
+ * costed with egg_mdl_cost; the search stops after the first clustering
+ * with a single cluster (or max_candidates, 0 = 256) and writes the labels
+ * of the clustering of least cost (the first on ties).  The reference
+ * clusters with its Python SynC instead (DynamicalClustering, allclose
+ * grouping); stats optional. */
+int egg_mdl_search(const float *x, int64_t n, int32_t d, int32_t k, int32_t max_candidates, int32_t *labels,
+                   egg_mdl_stats *stats, void *stream);
 
 #ifdef __cplusplus
 }

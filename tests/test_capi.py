@@ -33,7 +33,7 @@ def test_exports_every_declared_symbol(eggsync_lib):
 
 
 def test_abi_version_and_status_names(eggsync_lib):
-    assert eggsync_lib.egg_abi_version() == 4
+    assert eggsync_lib.egg_abi_version() == 5
     # the normal build collects no interaction counters
     buf = (C.c_int64 * 16)()
     assert eggsync_lib.egg_update_counters(buf, 16) == 0
@@ -51,7 +51,9 @@ def test_struct_layout_matches_header(tmp_path):
               ("egg_mlp", _lib.EggMlp, ["min_count", "w1", "b3"]),
               ("egg_mlp_train_opts", _lib.EggMlpTrainOpts, ["lr", "seed"]),
               ("egg_batch_item", _lib.EggBatchItem, ["n", "eps", "labels", "status"]),
-              ("egg_batch_stats", _lib.EggBatchStats, ["workspace_bytes", "total_ms", "tune_ms", "itr_ms"])]
+              ("egg_batch_stats", _lib.EggBatchStats, ["workspace_bytes", "total_ms", "tune_ms", "itr_ms"]),
+              ("egg_mdl_stats", _lib.EggMdlStats, ["eps_step", "candidates", "end_reason", "cost_best", "cap",
+                                                  "costs", "clusters"])]
     body = "".join('printf("%%zu\\n", sizeof(%s));' % t + "".join(
         'printf("%%zu\\n", offsetof(%s, %s));' % (t, f) for f in fs) for t, _, fs in fields)
     src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "eggsync.h"\nint main(){%s}\n' % body)
@@ -133,6 +135,25 @@ def test_normalize_argument_errors(eggsync_lib):
     assert L.egg_minmax_normalize(None, 10, 2, xp, None, None, None) == _lib.EGG_ERR_ARG
     assert L.egg_minmax_normalize(xp, 0, 2, xp, None, None, None) == _lib.EGG_ERR_ARG
     assert L.egg_minmax_normalize(xp, 10, 65, xp, None, None, None) == _lib.EGG_ERR_ARG
+
+
+def test_mdl_argument_errors(eggsync_lib):
+    L = eggsync_lib
+    x = np.zeros((10, 2), np.float32)
+    lab = np.zeros(10, np.int32)
+    xp, lp = C.c_void_p(x.ctypes.data), C.c_void_p(lab.ctypes.data)
+    out = (C.c_double * 2)()
+    cost = C.c_double()
+    assert L.egg_knn_mean(None, 10, 2, 3, out, None) == _lib.EGG_ERR_ARG
+    assert L.egg_knn_mean(xp, 10, 2, 0, out, None) == _lib.EGG_ERR_ARG      # k < 1
+    assert L.egg_knn_mean(xp, 10, 2, 32, out, None) == _lib.EGG_ERR_ARG     # k > 31
+    assert L.egg_knn_mean(xp, 4, 2, 3, out, None) == _lib.EGG_ERR_ARG       # n < k + 2
+    assert L.egg_knn_mean(xp, 10, 65, 3, out, None) == _lib.EGG_ERR_ARG
+    assert L.egg_mdl_cost(xp, 10, 2, None, C.byref(cost), None, None) == _lib.EGG_ERR_ARG
+    assert L.egg_mdl_cost(xp, 1, 2, lp, C.byref(cost), None, None) == _lib.EGG_ERR_ARG
+    assert L.egg_mdl_search(xp, 10, 2, 0, 0, lp, None, None) == _lib.EGG_ERR_ARG
+    assert L.egg_mdl_search(xp, 10, 2, 3, -1, lp, None, None) == _lib.EGG_ERR_ARG
+    assert L.egg_mdl_search(xp, 10, 2, 3, 0, None, None, None) == _lib.EGG_ERR_ARG
 
 
 def test_python_front_end_rejects_bad_input(eggsync_lib):

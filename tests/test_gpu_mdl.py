@@ -1,0 +1,109 @@
+"""The MDL eps search on the GPU (egg_knn_mean, egg_mdl_cost, egg_mdl_search)
+against the oracle (oracle/mdl_oracle.py) and the reference's own values
+(tests/golden/ref_mdl.npz).
+
+Bars: k-NN means within 1e-5 relative of the FP64 oracle and of the
+reference (FP32 distances); costs within 1e-6 relative (FP32 kernel
+exponent, FP64 sums); the search's eps values bit-exact to the float32
+schedule, its costs and cluster counts those of independent egg_sync runs
+at the same eps, its stop and argmin rules the reference's."""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from eggsync import data, egg_sync, knn_mean, mdl_cost, mdl_search
+import mdl_oracle as M
+
+pytestmark = pytest.mark.gpu
+
+REF = np.load(GOLDEN / "ref_mdl.npz")
+
+
+def blobs(seed, n, d, k=4, std=0.03, noise=0.05):
+    rng = np.random.default_rng(seed)
+    return data.blobs(rng, n, d, rng.uniform(0.2, 0.8, (k, d)), [std] * k, np.ones(k), noise)
+
+
+@pytest.mark.parametrize("d", (1, 2, 3, 5, 7))
+@pytest.mark.parametrize("k", (1, 4, 15, 31))
+def test_knn_mean_matches_oracle(d, k):
+    X = blobs(10 + d, 700, d)
+    a, b = knn_mean(X, k)
+    assert a == pytest.approx(M.nn_mean(X, k), rel=1e-5)
+    assert b == pytest.approx(M.nn_mean(X, k + 1), rel=1e-5)
+
+
+@pytest.mark.parametrize("name", ("s0", "s1", "s2", "s3"))
+def test_against_reference_values(name):
+    X, lab = REF[name + "_X"], REF[name + "_labels"]
+    for k in (1, 2, 3, 5):
+        assert knn_mean(X, k)[0] == pytest.approx(float(REF["%s_nn%d" % (name, k)]), rel=1e-5)
+    cost, K = mdl_cost(X, lab)
+    assert K == len(M.clusters_of(lab))
+    assert cost == pytest.approx(float(REF[name + "_cost"]), rel=1e-6)
+
+
+@pytest.mark.parametrize("d,eps", ((2, 0.03), (3, 0.05), (5, 0.12)))
+def test_cost_of_egg_sync_clusterings(d, eps):
+    torch = pytest.importorskip("torch")
+    X = blobs(20 + d, 3000, d)
+    lab, info = egg_sync(X, eps)
+    cost, K = mdl_cost(X, lab)
+    assert K == info["n_clusters"] == len(M.clusters_of(lab))
+    assert cost == pytest.approx(M.mdl_cost(X, lab), rel=1e-6)
+    # device inputs give the same bits; the cost is reproducible run to run
+    cd, Kd = mdl_cost(torch.from_numpy(X).cuda(), torch.from_numpy(lab).cuda())
+    assert (cd, Kd) == (cost, K)
+    assert mdl_cost(X, lab) == (cost, K)
+
+
+def test_cost_all_outliers_and_one_cluster():
+    X = blobs(31, 400, 2)
+    n = len(X)
+    for lab in (np.full(n, -1, np.int32), np.zeros(n, np.int32)):
+        cost, K = mdl_cost(X, lab)
+        assert K == len(M.clusters_of(lab))
+        assert cost == pytest.approx(M.mdl_cost(X, lab), rel=1e-6)
+
+
+def _check_search(X, k, cap):
+    lab, info = mdl_search(X, k, max_candidates=cap)
+    assert info["eps0"] == pytest.approx(M.nn_mean(X, k), rel=1e-5)
+    assert info["eps1"] == pytest.approx(M.nn_mean(X, k + 1), rel=1e-5)
+    # the float32 schedule, from the reported means
+    e = np.float32(info["eps0"])
+    step = np.float32(info["eps1"]) - e
+    assert np.float32(info["eps_step"]) == step
+    m = info["candidates"]
+    for c in range(m):
+        assert np.float32(info["eps"][c]) == e
+        lab_c, inf_c = egg_sync(X, float(e))
+        assert info["clusters"][c] == inf_c["n_clusters"]
+        assert info["costs"][c] == pytest.approx(M.mdl_cost(X, lab_c), rel=1e-6)
+        if c == info["best"]:
+            assert np.array_equal(lab, lab_c)
+        e = np.float32(e + step)
+    # stop rule and argmin (first minimum)
+    ks = info["clusters"]
+    assert all(v != 1 for v in ks[:-1])
+    if info["end_reason"] == "one cluster":
+        assert ks[-1] == 1
+    else:
+        assert info["end_reason"] == "candidate cap" and m == cap
+    assert info["best"] == int(np.argmin(info["costs"]))
+    assert info["cost_best"] == info["costs"][info["best"]]
+    assert info["n_clusters"] == ks[info["best"]]
+    return info
+
+
+def test_search_reaches_one_cluster():
+    rng = np.random.default_rng(41)
+    X = np.clip(0.5 + rng.normal(0, 0.04, (150, 2)), 0, 1).astype(np.float32)
+    info = _check_search(X, 31, 64)
+    assert info["end_reason"] == "one cluster"
+
+
+def test_search_candidate_cap():
+    X = blobs(42, 1500, 3, k=5)
+    info = _check_search(X, 5, 12)
+    assert info["end_reason"] == "candidate cap" and info["candidates"] == 12
