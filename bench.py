@@ -258,6 +258,7 @@ def run_ours(args, rank, local, world, pg):
     _, pinfo = egg_sync(Xd, eps, labels_out=lab_d, profile=True)
     learned = learned_leg(args, timed, Xd, eps, lab_d, dev) if world == 1 and not args.no_extra else None
     sweep = batched_sweep(dev) if world == 1 and not args.no_extra else None
+    mdl = mdl_leg(dev) if world == 1 and not args.no_extra else None
 
     ms = statistics.mean(dev_times)
     ms_e2e = statistics.mean(e2e_times)
@@ -315,6 +316,8 @@ def run_ours(args, rank, local, world, pg):
         line["learned"] = learned
     if sweep is not None:
         line["batched_sweep"] = sweep
+    if mdl is not None:
+        line["mdl_search"] = mdl
     return line
 
 
@@ -392,6 +395,48 @@ def batched_sweep(dev):
             "batched_s": min(tb), "sequential_s": ts, "speedup": ts / min(tb), "identical_to_sequential": same,
             "loop_iterations": bi["loop_iterations"], "launch_config": {k: bi[k] for k in (
                 "update_threads", "blocks_per_sm", "order")}}
+
+
+def mdl_leg(dev):
+    """The MDL eps search (Sync, python/SynCTorch.py:349-372) on 100k x 3D
+    (the first 100k points of the c2 shape), k = 5: the brute-force k-NN
+    kernel against the FP32 CUDA-core peak, one coding cost, and a search
+    capped at 16 candidates; device inputs, CUDA events around each call."""
+    import torch
+
+    from eggsync import data, egg_sync, knn_mean, mdl_cost, mdl_search
+
+    X = torch.from_numpy(data.c2(0)["X"][:100_000].copy()).to(dev)
+    n, d = X.shape
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn, reps):
+        fn()
+        ts = []
+        for _ in range(reps):
+            torch.cuda.synchronize(dev)
+            ev[0].record()
+            out = fn()
+            ev[1].record()
+            torch.cuda.synchronize(dev)
+            ts.append(ev[0].elapsed_time(ev[1]))
+        return min(ts), out
+
+    knn_ms, nn = timed(lambda: knn_mean(X, 5), 3)
+    lab, _ = egg_sync(X, 0.02)
+    cost_ms, (cost, K) = timed(lambda: mdl_cost(X, lab), 3)
+    search_ms, (_, info) = timed(lambda: mdl_search(X, 5, max_candidates=16), 1)
+    # per pair: d subtractions and d fused multiply-adds (3d FLOP)
+    flops = float(n) * n * 3 * d
+    fp32_peak = 148 * 128 * 2 * 1.965e9  # nominal FP32 CUDA-core FLOP/s at the max SM clock
+    return {"workload": "100k x 3D (c2 shape, first 100k points), k = 5, at most 16 candidates",
+            "knn_ms": knn_ms, "knn_pairs_per_s": n * n / (knn_ms * 1e-3),
+            "knn_roofline": {"bound": "fp32", "achieved": flops / (knn_ms * 1e-3) / 1e12,
+                             "peak": fp32_peak / 1e12, "unit": "TFLOP/s",
+                             "frac": flops / (knn_ms * 1e-3) / fp32_peak, "peak_source": "nominal"},
+            "nn_k": nn[0], "nn_k1": nn[1], "cost_ms": cost_ms, "cost": cost, "cost_clusters": K,
+            "search_ms": search_ms, "candidates": info["candidates"], "best": info["best"],
+            "eps_best": info["eps_best"], "n_clusters": info["n_clusters"], "end_reason": info["end_reason"]}
 
 
 def run_reference(args, rank, world):

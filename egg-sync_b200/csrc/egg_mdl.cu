@@ -397,26 +397,71 @@ std::vector<double> bandwidths(Arena& A, const float* xd, int n, int d, cudaStre
 //   L_D = -( sum_C sum_{x in C} log2(f(x) / sum_{y in C} f(y))
 //            + outliers * (2 pi)^(-1/2) * prod h )
 // Returns L_M + L_D; *clusters = number of clusters.
-double mdl_cost(Arena& A, const float* xd, int n, int d, const int* labels_d, const std::vector<double>& h,
-                int* clusters, cudaStream_t st) {
-    unsigned* keys = A.get<unsigned>(n);
-    unsigned* keys_s = A.get<unsigned>(n);
-    int* idx = A.get<int>(n);
-    int* idx_s = A.get<int>(n);
-    int* bad = A.get<int>(1);
+// Device arrays of the cost of labellings of one n x d input, sized once
+// (the search costs every candidate with the same arrays).
+struct CostWs {
+    Arena A;
+    int n, d;
+    unsigned *keys, *keys_s;
+    int *idx, *idx_s, *head, *iota, *incl, *seg, *begin, *scal;  // scal: bad flag, m, K
+    float *xs, *invh;
+    double *f, *lf, *sf, *slf;
+    void* tmp = nullptr;
+    size_t tmp_bytes = 0;
+    CostWs(int n_, int d_) : n(n_), d(d_) {
+        keys = A.get<unsigned>(n);
+        keys_s = A.get<unsigned>(n);
+        idx = A.get<int>(n);
+        idx_s = A.get<int>(n);
+        head = A.get<int>(n);
+        iota = A.get<int>(n);
+        incl = A.get<int>(n);
+        seg = A.get<int>(n);
+        begin = A.get<int>((size_t)n + 1);
+        scal = A.get<int>(4);
+        xs = A.get<float>((size_t)n * d);
+        invh = A.get<float>(d);
+        f = A.get<double>(n);
+        lf = A.get<double>(n);
+        sf = A.get<double>(n);
+        slf = A.get<double>(n);
+    }
+    // CUB's two-phase calls with one growing scratch buffer
+    template <typename F>
+    void cub(F&& fn) {
+        size_t bytes = 0;
+        EGG_CHECK(fn(nullptr, bytes));
+        if (bytes > tmp_bytes) {
+            tmp = A.get<char>(bytes);
+            tmp_bytes = bytes;
+        }
+        EGG_CHECK(fn(tmp, bytes));
+    }
+};
+
+// Coding cost of one labelling (device labels, original order), L_Clust_Outl:
+//   L_M = sum_C |C| log2(n / |C|) + d/2 log2 |C|  +  outliers * log2 n
+//   L_D = -( sum_C sum_{x in C} log2(f(x) / sum_{y in C} f(y))
+//            + outliers * (2 pi)^(-1/2) * prod h )
+// Returns L_M + L_D; *clusters = number of clusters.
+double mdl_cost(CostWs& W, const float* xd, const int* labels_d, const std::vector<double>& h, int* clusters,
+                cudaStream_t st) {
+    const int n = W.n, d = W.d;
+    int* bad = W.scal;
+    int* dm = W.scal + 1;
+    int* nseg = W.scal + 2;
     EGG_CHECK(cudaMemsetAsync(bad, 0, 4, st));
-    k_label_keys<<<grid_for((size_t)n, 256), 256, 0, st>>>(labels_d, n, keys, idx, bad);
-    cub_call(A, [&](void* t, size_t& b) {
-        return cub::DeviceRadixSort::SortPairs(t, b, keys, keys_s, idx, idx_s, n, 0, 32, st);
+    k_label_keys<<<grid_for((size_t)n, 256), 256, 0, st>>>(labels_d, n, W.keys, W.idx, bad);
+    W.cub([&](void* t, size_t& b) {
+        return cub::DeviceRadixSort::SortPairs(t, b, W.keys, W.keys_s, W.idx, W.idx_s, n, 0, 32, st);
     });
     // clustered points: keys below 0xffffffff
-    int* dm = A.get<int>(1);
-    k_first_outlier<<<1, 1, 0, st>>>(keys_s, n, dm);
-    int m = 0, hbad = 0;
-    EGG_CHECK(cudaMemcpyAsync(&m, dm, 4, cudaMemcpyDeviceToHost, st));
-    EGG_CHECK(cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, st));
+    k_first_outlier<<<1, 1, 0, st>>>(W.keys_s, n, dm);
+    int hs2[2];
+    EGG_CHECK(cudaMemcpyAsync(hs2, bad, 8, cudaMemcpyDeviceToHost, st));
     EGG_CHECK(cudaStreamSynchronize(st));
-    if (hbad) throw ArgError{EGG_ERR_ARG, "labels must be -1 (outlier) or a cluster id >= 0"};
+    if (hs2[0]) throw ArgError{EGG_ERR_ARG, "labels must be -1 (outlier) or a cluster id >= 0"};
+    const int m = hs2[1];
     const int outliers = n - m;
     double LM = (double)outliers * std::log2((double)n);
     double prodh = 1.0;
@@ -424,47 +469,40 @@ double mdl_cost(Arena& A, const float* xd, int n, int d, const int* labels_d, co
     double LD = (double)outliers * std::pow(2.0 * M_PI, -0.5) * prodh;
     *clusters = 0;
     if (m > 0) {
-        int* head = A.get<int>(m);
-        int* iota = A.get<int>(m);
-        int* incl = A.get<int>(m);
-        int* seg = A.get<int>(m);
-        int* begin = A.get<int>(m + 1);
-        int* nseg = A.get<int>(1);
-        k_heads<<<grid_for((size_t)m, 256), 256, 0, st>>>(keys_s, m, head, iota);
-        cub_call(A, [&](void* t, size_t& b) {
-            return cub::DeviceSelect::Flagged(t, b, iota, head, begin, nseg, m, st);
+        k_heads<<<grid_for((size_t)m, 256), 256, 0, st>>>(W.keys_s, m, W.head, W.iota);
+        W.cub([&](void* t, size_t& b) {
+            return cub::DeviceSelect::Flagged(t, b, W.iota, W.head, W.begin, nseg, m, st);
         });
-        cub_call(A, [&](void* t, size_t& b) { return cub::DeviceScan::InclusiveSum(t, b, head, incl, m, st); });
-        k_seg_of<<<grid_for((size_t)m, 256), 256, 0, st>>>(incl, m, seg);
+        W.cub([&](void* t, size_t& b) { return cub::DeviceScan::InclusiveSum(t, b, W.head, W.incl, m, st); });
+        k_seg_of<<<grid_for((size_t)m, 256), 256, 0, st>>>(W.incl, m, W.seg);
+        k_gather_sorted<<<grid_for((size_t)m * d, 256), 256, 0, st>>>(xd, d, W.idx_s, m, W.xs);
         int K = 0;
         EGG_CHECK(cudaMemcpyAsync(&K, nseg, 4, cudaMemcpyDeviceToHost, st));
         EGG_CHECK(cudaStreamSynchronize(st));
-        EGG_CHECK(cudaMemcpyAsync(begin + K, &m, 4, cudaMemcpyHostToDevice, st));
-        EGG_CHECK(cudaStreamSynchronize(st));
-        float* xs = A.get<float>((size_t)m * d);
-        k_gather_sorted<<<grid_for((size_t)m * d, 256), 256, 0, st>>>(xd, d, idx_s, m, xs);
-        std::vector<float> ihh(d);
-        for (int l = 0; l < d; l++) ihh[l] = (float)(1.0 / h[l]);
-        float* invh = A.get<float>(d);
-        EGG_CHECK(cudaMemcpyAsync(invh, ihh.data(), 4 * (size_t)d, cudaMemcpyHostToDevice, st));
+        // begin[K] = m and the inverse bandwidths, one small upload
+        std::vector<int> up(1 + d);
+        up[0] = m;
+        for (int l = 0; l < d; l++) {
+            const float ih = (float)(1.0 / h[l]);
+            memcpy(&up[1 + l], &ih, 4);
+        }
+        EGG_CHECK(cudaMemcpyAsync(W.begin + K, up.data(), 4, cudaMemcpyHostToDevice, st));
+        EGG_CHECK(cudaMemcpyAsync(W.invh, up.data() + 1, 4 * (size_t)d, cudaMemcpyHostToDevice, st));
         const double norm = std::pow(2.0 * M_PI, -0.5 * d) / prodh;
-        double* f = A.get<double>(m);
-        double* lf = A.get<double>(m);
-        EGG_MDL_DISPATCH_D(d, k_kde, <<<(m + 255) / 256, 256, 0, st>>>(xs, m, d, seg, begin, invh, norm, f, lf));
+        EGG_MDL_DISPATCH_D(d, k_kde, <<<(m + 255) / 256, 256, 0, st>>>(W.xs, m, d, W.seg, W.begin, W.invh, norm,
+                                                                         W.f, W.lf));
         EGG_CHECK(cudaGetLastError());
-        double* sf = A.get<double>(K);
-        double* slf = A.get<double>(K);
-        cub_call(A, [&](void* t, size_t& b) {
-            return cub::DeviceSegmentedReduce::Sum(t, b, f, sf, K, begin, begin + 1, st);
+        W.cub([&](void* t, size_t& b) {
+            return cub::DeviceSegmentedReduce::Sum(t, b, W.f, W.sf, K, W.begin, W.begin + 1, st);
         });
-        cub_call(A, [&](void* t, size_t& b) {
-            return cub::DeviceSegmentedReduce::Sum(t, b, lf, slf, K, begin, begin + 1, st);
+        W.cub([&](void* t, size_t& b) {
+            return cub::DeviceSegmentedReduce::Sum(t, b, W.lf, W.slf, K, W.begin, W.begin + 1, st);
         });
         std::vector<int> hb(K + 1);
         std::vector<double> hs(K), hl(K);
-        EGG_CHECK(cudaMemcpyAsync(hb.data(), begin, 4 * (size_t)(K + 1), cudaMemcpyDeviceToHost, st));
-        EGG_CHECK(cudaMemcpyAsync(hs.data(), sf, 8 * (size_t)K, cudaMemcpyDeviceToHost, st));
-        EGG_CHECK(cudaMemcpyAsync(hl.data(), slf, 8 * (size_t)K, cudaMemcpyDeviceToHost, st));
+        EGG_CHECK(cudaMemcpyAsync(hb.data(), W.begin, 4 * (size_t)(K + 1), cudaMemcpyDeviceToHost, st));
+        EGG_CHECK(cudaMemcpyAsync(hs.data(), W.sf, 8 * (size_t)K, cudaMemcpyDeviceToHost, st));
+        EGG_CHECK(cudaMemcpyAsync(hl.data(), W.slf, 8 * (size_t)K, cudaMemcpyDeviceToHost, st));
         EGG_CHECK(cudaStreamSynchronize(st));
         for (int c = 0; c < K; c++) {
             const double sz = (double)(hb[c + 1] - hb[c]);
@@ -500,6 +538,7 @@ void mdl_search(const float* x, int n, int d, int k, int max_cand, int* labels, 
         throw ArgError{EGG_ERR_INPUT, "NN(k+1) equals NN(k): the eps schedule does not advance"};
     int* lab = A.get<int>((size_t)kMdlBatch * n);
     int* best_lab = A.get<int>(n);
+    CostWs W(n, d);
     float eps = e0;
     bool done = false;
     while (!done && R.candidates < max_cand) {
@@ -531,11 +570,7 @@ void mdl_search(const float* x, int n, int d, int k, int max_cand, int* labels, 
             const egg_batch_item& it = items[b];
             if (it.status < 0) throw ArgError{it.status, "clustering at eps " + std::to_string(it.eps) + " failed"};
             int K = 0;
-            double cost;
-            {
-                Arena C;
-                cost = mdl_cost(C, xd, n, d, it.labels, h, &K, st);
-            }
+            const double cost = mdl_cost(W, xd, it.labels, h, &K, st);
             R.costs.push_back(cost);
             R.eps.push_back(it.eps);
             R.ks.push_back(K);
@@ -595,8 +630,9 @@ extern "C" __attribute__((visibility("default"))) int egg_mdl_cost(const float* 
             ld = t;
         }
         const std::vector<double> h = egg::bandwidths(A, xd, (int)n, d, st);
+        egg::CostWs W((int)n, d);
         int K = 0;
-        *cost = egg::mdl_cost(A, xd, (int)n, d, ld, h, &K, st);
+        *cost = egg::mdl_cost(W, xd, ld, h, &K, st);
         if (clusters) *clusters = K;
         return EGG_OK;
     });
