@@ -23,8 +23,19 @@ float32 row-major layout, and draw everything else from
   U[0.005,0.03], equal sizes, 10% noise; eps 0.015.
 * ``train`` 100,000 x 3: 8-40 Gaussians, std U[0.005,0.03], 10% noise;
   eps 0.02 (seeds >= 1,000,000, disjoint from evaluation seeds).
+
+Real data sets: the reference's experiments cluster ten UCI-style files from
+its ``data/`` directory, min-max normalised, at eps 0.05
+(run_experiment.py:12, 53-62, 547-551; loaders python/data.py:44-97; the
+Roads file 3D_spatial_network.txt is not shipped with it).  Their points are
+not part of this package: ``load_real`` reads those files from a directory
+the caller names, with the reference's columns and delimiters, and
+``stand_in`` draws seeded points of the same shape (8 Gaussians with std
+U[0.02, 0.08], 5% noise), which the tests run through the GPU path.
 """
 from __future__ import annotations
+
+from pathlib import Path
 
 import numpy as np
 
@@ -138,3 +149,34 @@ def c4(seed=0, instances=64):
 
 
 CONFIGS = {"c1": c1, "c2": c2, "c3a": c3a, "c3b": c3b, "c5": c5}
+
+
+# name: (file in the reference's data/ directory, numpy.loadtxt arguments, (n, d))
+REAL = {
+    "banknote": ("data_banknote_authentication.txt", {"delimiter": ",", "usecols": (0, 1, 2, 3)}, (1372, 4)),
+    "yeast": ("yeast.data", {"usecols": (1, 2, 3, 4, 5, 6, 7, 8)}, (1484, 8)),
+    "wilt": ("wilt.data", {"delimiter": ",", "usecols": (1, 2, 3, 4, 5)}, (4839, 5)),
+    "ccpp": ("CCPP.data", {"delimiter": "\t", "skiprows": 1}, (9568, 5)),
+    "eb": ("eb.arff", {"delimiter": ",", "usecols": (0, 1, 4)}, (45781, 3)),
+    "skin_nonskin": ("Skin_NonSkin.txt", {"usecols": (0, 1, 2)}, (245057, 3)),
+    "eeg_eye_state": ("EEG Eye State.arff", {"delimiter": ",", "usecols": tuple(range(14))}, (14980, 14)),
+    "letter": ("letter-recognition.data", {"delimiter": ",", "usecols": tuple(range(1, 17))}, (20000, 16)),
+    "iris": ("iris.data", {"delimiter": ","}, (150, 4)),
+    "pendigits": ("pendigits.tra", {"delimiter": ","}, (7494, 17)),
+}
+REAL_EPS = 0.05
+
+
+def load_real(name, data_dir):
+    """One of the reference's real data sets from ``data_dir`` (a copy of its
+    data/ directory), min-max normalised, float32 (python/data.py:44-103)."""
+    f, kw, _ = REAL[name]
+    return min_max_normalize(np.loadtxt(Path(data_dir) / f, **kw))
+
+
+def stand_in(name, seed=0):
+    """Seeded synthetic points with the shape of real data set ``name``."""
+    n, d = REAL[name][2]
+    rng = np.random.default_rng(seed)
+    k = 8
+    return blobs(rng, n, d, rng.uniform(0.2, 0.8, (k, d)), rng.uniform(0.02, 0.08, k), np.ones(k), 0.05)
