@@ -30,7 +30,7 @@ enum Shape : int {
     kShapeOuter,       // ceil((n_outer + 1) / 256)
     kShapeCapN256,     // min(ceil(n / 256), 148 * 8)
     kShapeCapN128,     // min(ceil(n / 128), 148 * 8)
-    kShapeCapOuter,    // min(ceil(n_outer / 256), 148 * 8)
+    kShapeCapOuter,    // min(ceil(n_outer / 64), 148 * 8): 8 outer cells per warp
     kShapeFix,         // min(ceil(ceil(n / 32) / 8), 148 * 8)
     kShapeCapN256L,    // min(ceil(n / 256), 148 * 16)
     kShapeN64,         // ceil(n / 64)
@@ -52,7 +52,7 @@ __host__ __device__ inline int shape_blocks(int shape, const Geom& g) {
         case kShapeOuter: return cdiv((long)g.n_outer + 1, 256);
         case kShapeCapN256: return cap(cdiv(g.n, 256), 148 * 8);
         case kShapeCapN128: return cap(cdiv(g.n, 128), 148 * 8);
-        case kShapeCapOuter: return cap(cdiv(g.n_outer, 256) > 0 ? cdiv(g.n_outer, 256) : 1, 148 * 8);
+        case kShapeCapOuter: return cap(cdiv(g.n_outer, 64) > 0 ? cdiv(g.n_outer, 64) : 1, 148 * 8);
         case kShapeFix: return cap(cdiv(cdiv(g.n, 32), 8), 148 * 8);
         case kShapeCapN256L: return cap(cdiv(g.n, 256), 148 * 16);
         case kShapeN64: return cdiv(g.n, 64);

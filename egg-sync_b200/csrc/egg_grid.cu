@@ -123,15 +123,23 @@ __device__ __forceinline__ void check_cells_body(const Geom& g, const Work& w, i
     const int d = D > 0 ? D : g.d;
     const bool valid = w.ctrl[kCtrlGridValid] != 0;
     bool changed = false;
+    // d <= 4: the cell's coordinates packed 16 bits each, one load per point
+    constexpr bool kKeyed = D >= 1 && D <= 4;
+    const bool keyed = kKeyed && w.cell_key != nullptr;
     for (int i = bx * blockDim.x + threadIdx.x; i < g.n; i += gx * blockDim.x) {
         const int c = valid ? w.cell_of[i] : 0;
         bool moved = false;
+        unsigned long long key = 0;
         for (int l = 0; l < d; l++) {
             const float x = w.Xn[(size_t)l * g.ns + i];
             moved |= __float_as_uint(x) != __float_as_uint(w.X[(size_t)l * g.ns + i]);
             w.X[(size_t)l * g.ns + i] = x;
-            if (valid) changed |= cell_dim(x, g) != w.cell_dims[(size_t)l * g.ns + c];
+            if (valid) {
+                if (keyed) key |= (unsigned long long)cell_dim(x, g) << (16 * l);
+                else changed |= cell_dim(x, g) != w.cell_dims[(size_t)l * g.ns + c];
+            }
         }
+        if (valid && keyed) changed |= key != w.cell_key[c];
         // per warp of sorted points: did any of them move?  (lane 0 of the
         // warp is active whenever any lane is: the warp's first index is < n)
         const unsigned m = __ballot_sync(__activemask(), moved);
@@ -577,6 +585,51 @@ __device__ void combine_big(const Geom& g, const Work& w, int c, int wh, int wt,
     }
 }
 
+// One field of one big spanning cell (0: sum sin, 1: sum 1 - cos, 2: min,
+// 3: max), the whole warp: lane L accumulates the partials of warps
+// wh + L, wh + L + 32, ... in that order, then a butterfly over the lanes --
+// the order combine_big uses, so the result is the same bit for bit.  The
+// four fields of a cell go to four warps, and each lane keeps kB partials
+// per dimension in flight: a cell over thousands of warps no longer holds
+// the launch on one warp's chain of loads.
+template <int D>
+__device__ void combine_big_field(const Geom& g, const Work& w, int c, int wh, int wt, int lane, int nw, int f) {
+    constexpr int kB = 48 / D > 0 ? 48 / D : 1;
+    const int d = D;
+    double acc[D];
+#pragma unroll
+    for (int l = 0; l < D; l++) acc[l] = f < 2 ? 0.0 : (f == 2 ? 1e300 : -1e300);
+    for (int k0 = wh + lane; k0 <= wt; k0 += 32 * kB) {
+        double v[kB][D];
+#pragma unroll
+        for (int u = 0; u < kB; u++) {
+            const int k = k0 + 32 * u;
+            const int kk = k <= wt ? k : k0;  // in-range stand-in, not accumulated
+            const int rec = (kk == wh) ? 1 : 0;
+#pragma unroll
+            for (int l = 0; l < D; l++) v[u][l] = w.wpart[wp_idx(f, l, d, rec, nw, kk)];
+        }
+#pragma unroll
+        for (int u = 0; u < kB; u++) {
+            if (k0 + 32 * u > wt) break;
+#pragma unroll
+            for (int l = 0; l < D; l++)
+                acc[l] = f < 2 ? acc[l] + v[u][l] : (f == 2 ? fmin(acc[l], v[u][l]) : fmax(acc[l], v[u][l]));
+        }
+    }
+    float* out = f == 0 ? w.css : (f == 1 ? w.csm : (f == 2 ? w.cbmin : w.cbmax));
+#pragma unroll
+    for (int l = 0; l < D; l++) {
+        double a = acc[l];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double b = __shfl_xor_sync(0xffffffffu, a, o);
+            a = f < 2 ? a + b : (f == 2 ? fmin(a, b) : fmax(a, b));
+        }
+        if (lane == 0) out[(size_t)l * g.ns + c] = (float)a;
+    }
+}
+
 // Cells spanning more than one warp: combine the warp partials in FP64 in a
 // fixed order.  Cells over four or more warps (the heavily populated ones)
 // get a warp each; the others (nearly all: a small cell straddling a warp
@@ -593,11 +646,21 @@ __device__ __forceinline__ void cell_sums_fix_body(const Geom& g, const Work& w,
     const int it = w.ctrl[kCtrlIter];
     const int big = w.ctrl[kCtrlBigCount];
     const int warps = (gx * blockDim.x) >> 5;
-    for (int e = (bx * blockDim.x + threadIdx.x) >> 5; e < big; e += warps) {
-        const int c = w.big_list[e];
-        if (!rebuilt && w.span_mark[c] != it) continue;  // uniform across the warp
-        const int wh = w.cell_start[c] >> 5, wt = (w.cell_start[c + 1] - 1) >> 5;
-        combine_big<D>(g, w, c, wh, wt, lane, nw);
+    if constexpr (D > 0) {
+        // a warp per (cell, field)
+        for (int e = (bx * blockDim.x + threadIdx.x) >> 5; e < 4 * big; e += warps) {
+            const int c = w.big_list[e >> 2];
+            if (!rebuilt && w.span_mark[c] != it) continue;  // uniform across the warp
+            const int wh = w.cell_start[c] >> 5, wt = (w.cell_start[c + 1] - 1) >> 5;
+            combine_big_field<D>(g, w, c, wh, wt, lane, nw, e & 3);
+        }
+    } else {
+        for (int e = (bx * blockDim.x + threadIdx.x) >> 5; e < big; e += warps) {
+            const int c = w.big_list[e];
+            if (!rebuilt && w.span_mark[c] != it) continue;  // uniform across the warp
+            const int wh = w.cell_start[c] >> 5, wt = (w.cell_start[c + 1] - 1) >> 5;
+            combine_big<D>(g, w, c, wh, wt, lane, nw);
+        }
     }
     const int count = w.ctrl[kCtrlSpanCount];
     for (int e = bx * blockDim.x + threadIdx.x; e < count; e += gx * blockDim.x) {

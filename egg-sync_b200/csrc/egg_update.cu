@@ -464,33 +464,37 @@ __global__ void __launch_bounds__(T) kb_update(BatchArgs B) {
 // r + 1 cells, for_candidates) can hold a moved point's old or new position.
 // The dirty marks are cleared as they are consumed, so the array is clean
 // again when the update after next writes it.
-// A warp reads 32 outer cells at once; the lanes share the stencil entries
-// of each dirty one (dirty cells cluster around the regions still moving, so
-// a thread per cell would leave a few SMs with all the atomics).
+// A warp reads kNeedChunk outer cells at once; the lanes share the stencil
+// entries of each dirty one (dirty cells cluster around the regions still
+// moving, so a long run of them per warp would hold the whole launch).
+// The dilation is closed-form: block b covers the blocks
+// [b - ceil((r+1)/zblk), b + 1 + floor(r/zblk)], clipped to [0, nzb).
+constexpr int kNeedChunk = 8;
+
 __device__ __forceinline__ void need_body(const Geom& g, const Work& w, int bx, int gx) {
     const int it = w.ctrl[kCtrlIter];
     unsigned long long* prev = w.dirty[(it + 1) & 1];
     const int nst = w.st_count[0];
     const int lane = threadIdx.x & 31;
-    // warp-uniform loop over chunks of 32 outer cells
-    for (int o0 = bx * blockDim.x + (threadIdx.x & ~31); o0 < g.n_outer; o0 += gx * blockDim.x) {
-        const int o = o0 + lane;
-        const unsigned long long mine = o < g.n_outer ? prev[o] : 0ull;
+    const int wpb = blockDim.x >> 5;
+    const int lo_sh = min(63, (g.r + g.zblk) / g.zblk), hi_sh = min(63, 1 + g.r / g.zblk);
+    const unsigned long long full = g.nzb >= 64 ? ~0ull : (1ull << g.nzb) - 1ull;
+    const long long stride = (long long)gx * wpb * kNeedChunk;
+    // warp-uniform loop over chunks of outer cells
+    for (long long o0 = ((long long)bx * wpb + (threadIdx.x >> 5)) * kNeedChunk; o0 < g.n_outer; o0 += stride) {
+        const long long o = o0 + lane;
+        const unsigned long long mine = (lane < kNeedChunk && o < g.n_outer) ? prev[o] : 0ull;
         if (mine) prev[o] = 0;
         unsigned todo = __ballot_sync(0xffffffffu, mine != 0);
         while (todo) {
             const int src = __ffs(todo) - 1;
             todo &= todo - 1;
-            unsigned long long m = __shfl_sync(0xffffffffu, mine, src);
-            const int oc = o0 + src;
+            const unsigned long long m = __shfl_sync(0xffffffffu, mine, src);
+            const int oc = (int)o0 + src;
             unsigned long long dil = 0;
-            while (m) {
-                const int b = __ffsll((long long)m) - 1;
-                m &= m - 1;
-                const int lo = max(0, b * g.zblk - g.r - 1);
-                const int hi = min(g.width - 1, (b + 1) * g.zblk - 1 + g.r + 1);
-                for (int k = lo / g.zblk; k <= hi / g.zblk; k++) dil |= 1ull << k;
-            }
+            for (int s = 0; s <= lo_sh; s++) dil |= m >> s;
+            for (int s = 1; s <= hi_sh; s++) dil |= m << s;
+            dil &= full;
             int co[32];
             int rem = oc;
             for (int l = 0; l < g.od; l++) {

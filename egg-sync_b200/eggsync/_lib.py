@@ -137,12 +137,15 @@ def load():
     L.egg_simple_sync_run.argtypes = [vp, C.c_int64, C.c_int32, C.c_float, C.c_float, C.c_int32, vp, vp,
                                       C.POINTER(EggStats), vp]
     L.egg_simple_sync_run.restype = C.c_int
-    L.egg_knn_mean.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, C.POINTER(C.c_double), vp]
-    L.egg_knn_mean.restype = C.c_int
-    L.egg_mdl_cost.argtypes = [vp, C.c_int64, C.c_int32, vp, C.POINTER(C.c_double), C.POINTER(C.c_int32), vp]
-    L.egg_mdl_cost.restype = C.c_int
-    L.egg_mdl_search.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, C.c_int32, vp, C.POINTER(EggMdlStats), vp]
-    L.egg_mdl_search.restype = C.c_int
+    # the eps search (ABI 5); an older library without it still loads, and
+    # calling the missing entry point raises AttributeError
+    if hasattr(L, "egg_mdl_search"):
+        L.egg_knn_mean.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, C.POINTER(C.c_double), vp]
+        L.egg_knn_mean.restype = C.c_int
+        L.egg_mdl_cost.argtypes = [vp, C.c_int64, C.c_int32, vp, C.POINTER(C.c_double), C.POINTER(C.c_int32), vp]
+        L.egg_mdl_cost.restype = C.c_int
+        L.egg_mdl_search.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, C.c_int32, vp, C.POINTER(EggMdlStats), vp]
+        L.egg_mdl_search.restype = C.c_int
     L.egg_minmax_normalize.argtypes = [vp, C.c_int64, C.c_int32, vp, vp, vp, vp]
     L.egg_minmax_normalize.restype = C.c_int
     L.egg_mlp_feature_dim.argtypes = [C.c_int32]
