@@ -23,7 +23,6 @@
 #include <cuda_runtime.h>
 
 #include <cub/device/device_radix_sort.cuh>
-#include <cub/device/device_reduce.cuh>
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_segmented_reduce.cuh>
 #include <cub/device/device_select.cuh>
@@ -31,7 +30,6 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <limits>
 #include <string>
 #include <vector>
 
