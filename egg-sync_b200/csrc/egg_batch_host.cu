@@ -128,8 +128,9 @@ __global__ void __launch_bounds__(1024) k_batch_ctl(CtlArgs a, int phase, cudaGr
             act = !done;
         }
         if (act) {
-            // k_iter_begin
+            // k_iter_begin (with the grid check's begin step)
             ctrl[kCtrlFlag] = 1;
+            ctrl[kCtrlChanged] = 0;
             w.stamps[4 * ctrl[kCtrlIter] + 0] = now;
         }
     }
@@ -207,12 +208,6 @@ __device__ __forceinline__ void load_body(const Geom& g, const Work& w, int bx, 
 
 __global__ void __launch_bounds__(256) kb_load(BatchArgs B) {
     batch_for(B, [&](const Geom& g, const Work& w, int bx, int gx) { load_body(g, w, bx, gx); });
-}
-
-__global__ void kb_mark_extra(BatchArgs B) {
-    batch_for(B, [&](const Geom&, const Work& w, int, int) {
-        if (threadIdx.x == 0 && w.ctrl[kCtrlFlag] != 0) atomicAdd(w.ctrl + kCtrlExtraRuns, 1);
-    });
 }
 
 __global__ void k_batch_results(const Work* works, int count, int* out) {
@@ -435,11 +430,11 @@ void set_tables(Plan& P, const Config& c) {
 void enqueue_group(Plan& P, int k, cudaStream_t st) {
     Group& gr = P.groups[k];
     const Exec ex = batched(gr.act, gr.d);
-    launch_build(ex, st);
+    launch_build_check(ex, st, false);  // the control kernel cleared the changed words
+    launch_build_sort(ex, st);
     launch_cell_sums(ex, st);
     launch_need(ex, st);
     launch_update(ex, nullptr, st);
-    kb_mark_extra<<<ex.blocks(kShapeOne, 32), 32, 0, st>>>(ex.args(kShapeOne));
     launch_extra_check(ex, st);
 }
 
@@ -760,9 +755,9 @@ int enqueue_prologue(State& S, Plan& P, int max_iter) {
     return launches + 1;
 }
 
-// kernels of one group's iteration: build, cell sums (2), need, update,
-// mark, extra check (3)
-int group_launches(const Group& gr) { return 3 * gr.act.max_passes + 6 + 2 + 1 + 1 + 1 + 3; }
+// kernels of one group's iteration: build (grid check, radix passes, 4
+// tables), cell sums (2), need, update, extra check (3)
+int group_launches(const Group& gr) { return 1 + 3 * gr.act.max_passes + 4 + 2 + 1 + 1 + 3; }
 
 // Kernels of the loop: gate and control every iteration, and each group's
 // kernels in the iterations where it had active instances (the largest

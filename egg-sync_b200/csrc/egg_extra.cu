@@ -103,6 +103,9 @@ __device__ __forceinline__ void ball_bbox_body(const Geom& g, const Work& w, int
     if (bx == 0 && threadIdx.x == 0) {
         const int it = w.ctrl[kCtrlIter];
         w.stamps[4 * it + 2] = globaltimer();
+        // the extra check runs in this iteration when the flag reached it
+        // (only the annulus kernel, launched after this one, clears the flag)
+        if (w.ctrl[kCtrlFlag] != 0) atomicAdd(w.ctrl + kCtrlExtraRuns, 1);
     }
     if (w.ctrl[kCtrlFlag] == 0) return;
     for (int i = bx * blockDim.x + threadIdx.x; i < g.n; i += gx * blockDim.x) {

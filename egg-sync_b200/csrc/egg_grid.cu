@@ -843,8 +843,8 @@ __global__ void k_unsort_int(Geom g, Work w, const int* __restrict__ src, int* _
         }                                                                                            \
     } while (0)
 
-void launch_build_check(const Exec& ex, cudaStream_t st) {
-    EGG_GO(ex, kShapeOne, 32, st, build_begin);
+void launch_build_check(const Exec& ex, cudaStream_t st, bool begin) {
+    if (begin) EGG_GO(ex, kShapeOne, 32, st, build_begin);
     EGG_GO_D(ex, kShapeCapN256, 256, st, check_cells);
 }
 

@@ -339,9 +339,11 @@ __global__ void k_ctrl_reset(Work w, int max_iter, int full_update) {
     }
 }
 
+// also opens the grid check (the build-begin step: no point seen leaving its cell yet)
 __global__ void k_iter_begin(Work w) {
     const int it = w.ctrl[kCtrlIter];
     w.ctrl[kCtrlFlag] = 1;
+    w.ctrl[kCtrlChanged] = 0;
     w.stamps[4 * it + 0] = globaltimer();
 }
 
@@ -361,11 +363,6 @@ __global__ void k_iter_end(Work w, cudaGraphConditionalHandle h, int in_graph, i
     if (in_graph && done) cudaGraphSetConditional(h, 0);
 }
 
-// whether the extra check ran in iteration `it` is visible as stamps[2] < stamps[3]
-// of that iteration; extra_checks counts flags that reached the extra check
-__global__ void k_mark_extra(Work w) {
-    if (w.ctrl[kCtrlFlag] != 0) atomicAdd(w.ctrl + kCtrlExtraRuns, 1);
-}
 
 // One iteration of the loop body.  With prof (8 events), the four kernel
 // groups are bracketed by CUDA events on the launching stream.
@@ -379,7 +376,7 @@ void enqueue_part(Instance& I, int part, cudaGraphConditionalHandle h, int in_gr
     if (part == 0) {
         k_iter_begin<<<1, 1, 0, st>>>(I.w);
         mark(0);
-        launch_build_check(single(I.g, I.w), st);
+        launch_build_check(single(I.g, I.w), st, false);
         return;
     }
     if (part == 1) {
@@ -395,7 +392,6 @@ void enqueue_part(Instance& I, int part, cudaGraphConditionalHandle h, int in_gr
     mark(4);
     launch_update(single(I.g, I.w), nullptr, st);
     mark(5);
-    k_mark_extra<<<1, 1, 0, st>>>(I.w);
     mark(6);
     launch_extra_check(single(I.g, I.w), st);
     mark(7);
@@ -657,15 +653,16 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
             stats->kernel_ms[k] = kms[k];
             stats->kernel_launches[k] = kl[k];
         }
-        // launches: reset + transpose; per iteration: begin, grid check (2),
+        // launches: reset + transpose; per iteration: begin, grid check,
         // grid sort (3 per radix pass + 4), 2 cell sums, need, [2 order
-        // parameter], update, mark, 3 extra check, end; then the final
-        // build, labels (1 or 4 kernels), [2 cell sums + 2 order parameter],
-        // [positions].  In the loop graph a gate kernel runs every iteration
-        // and the grid sort only in iterations where some point changed cell.
+        // parameter], update, 3 extra check, end; then the final build
+        // (begin, check, sort), labels (1 or 4 kernels), [2 cell sums + 2
+        // order parameter], [positions].  In the loop graph a gate kernel
+        // runs every iteration and the grid sort only in iterations where
+        // some point changed cell.
         const int sort_l = 3 * plan_count(g) + 4;
         const int build_l = sort_l + 2;
-        const int per_iter = build_l + 10 + ((g.order_mode == 2 || g.stop_rule == 1) ? 2 : 0);
+        const int per_iter = sort_l + 1 + 9 + ((g.order_mode == 2 || g.stop_rule == 1) ? 2 : 0);
         const int final_l = build_l + (opts.labels_mode == 1 ? 1 : 4) + (g.order_mode == 1 ? 4 : 0) +
                             (opts.positions_out ? 1 : 0);
         long long loop_l = (long long)iters * per_iter;

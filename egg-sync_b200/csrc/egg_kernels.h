@@ -70,8 +70,9 @@ inline Exec batched(const BatchTables& bt, int d) {
 // the grid of the current positions Xn (radix passes: plan_count/plan_pass)
 void launch_build(const Exec& ex, cudaStream_t st);
 // its two halves: has any point left its cell (copies the positions), and
-// the sort and cell tables, whose kernels return at once when none has
-void launch_build_check(const Exec& ex, cudaStream_t st);
+// the sort and cell tables, whose kernels return at once when none has.
+// begin = false: the caller's loop control already cleared the changed word.
+void launch_build_check(const Exec& ex, cudaStream_t st, bool begin = true);
 void launch_build_sort(const Exec& ex, cudaStream_t st);
 void launch_cell_sums(const Exec& ex, cudaStream_t st);
 void launch_transpose_in(const Geom& g, const Work& w, const float* x, cudaStream_t st);
