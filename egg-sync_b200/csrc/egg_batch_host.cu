@@ -108,6 +108,7 @@ __global__ void __launch_bounds__(1024) k_batch_ctl(CtlArgs a, int phase, cudaGr
     const int t = threadIdx.x;
     const unsigned long long now = globaltimer();
     bool act = false;
+    bool left = false;  // this instance finished in this call
     if (t < a.count) {
         const Work& w = a.works[t];
         int* ctrl = w.ctrl;
@@ -126,6 +127,7 @@ __global__ void __launch_bounds__(1024) k_batch_ctl(CtlArgs a, int phase, cudaGr
             const int done = flag != 0 || next >= ctrl[kCtrlMaxIter];
             ctrl[kCtrlDone] = done;
             act = !done;
+            left = done;
         }
         if (act) {
             // k_iter_begin (with the grid check's begin step)
@@ -134,8 +136,13 @@ __global__ void __launch_bounds__(1024) k_batch_ctl(CtlArgs a, int phase, cudaGr
             w.stamps[4 * ctrl[kCtrlIter] + 0] = now;
         }
     }
+    // The active lists and block offsets change only when an instance
+    // finishes: otherwise those of the last call stand.
+    const bool rebuild = __syncthreads_or(phase == 0 || left) != 0;
     int any = 0;
-    for (int k = 0; k < a.ngroups; k++) {
+    if (!rebuild)
+        for (int k = 0; k < a.ngroups; k++) any += a.nact[k];
+    for (int k = 0; rebuild && k < a.ngroups; k++) {
         const bool mine = act && t >= a.gstart[k] && t < a.gstart[k + 1];
         int v[kNumSlots], tot[kNumSlots];
         v[0] = mine ? 1 : 0;
