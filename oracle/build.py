@@ -18,8 +18,8 @@
   ``-fopenmp``/libgomp link.  The reference's own build (a torch JIT
   ``load``) is not run.
 
-The outputs are git-ignored but travel with the repository snapshot, so the
-GPU box uses the files built here (``/root/reference`` does not exist there).
+The outputs are git-ignored but travel with copies of the working tree, so a
+machine without the reference tree uses the files built here.
 """
 from __future__ import annotations
 
