@@ -43,7 +43,7 @@ def test_against_reference_values(name):
     assert cost == pytest.approx(float(REF[name + "_cost"]), rel=1e-6)
 
 
-@pytest.mark.parametrize("d,eps", ((2, 0.03), (3, 0.05), (5, 0.12)))
+@pytest.mark.parametrize("d,eps", ((2, 0.03), (3, 0.05), (5, 0.12), (7, 0.2)))  # d = 7: generic-d kernels
 def test_cost_of_egg_sync_clusterings(d, eps):
     torch = pytest.importorskip("torch")
     X = blobs(20 + d, 3000, d)
@@ -107,3 +107,13 @@ def test_search_candidate_cap():
     X = blobs(42, 1500, 3, k=5)
     info = _check_search(X, 5, 12)
     assert info["end_reason"] == "candidate cap" and info["candidates"] == 12
+
+
+def test_search_device_input_same_result():
+    torch = pytest.importorskip("torch")
+    X = blobs(43, 1200, 2, k=3)
+    lab, info = mdl_search(X, 4, max_candidates=6)
+    out = torch.empty(len(X), dtype=torch.int32, device="cuda")
+    lab_d, info_d = mdl_search(torch.from_numpy(X).cuda(), 4, max_candidates=6, labels_out=out)
+    assert np.array_equal(lab, out.cpu().numpy())
+    assert info_d["costs"] == info["costs"] and info_d["eps"] == info["eps"]
