@@ -111,6 +111,18 @@ def dist_setup(args):
     return rank, local, world, pg
 
 
+def max_over_ranks(pg, vals, device):
+    """Each value's maximum over the ranks (an all-reduce MAX); the values
+    themselves with one rank.  Every rank gets the result."""
+    if pg is None:
+        return [float(v) for v in vals]
+    import torch
+
+    t = torch.tensor([float(v) for v in vals], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 class Clocks:
     """nvidia-smi sampling during the timed region."""
 
@@ -262,12 +274,7 @@ def run_ours(args, rank, local, world, pg):
 
     ms = statistics.mean(dev_times)
     ms_e2e = statistics.mean(e2e_times)
-    t_max = ms
-    t_e2e_max = ms_e2e
-    if pg is not None:
-        t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        t_max, t_e2e_max = float(t[0]), float(t[1])
+    t_max, t_e2e_max = max_over_ranks(pg, [ms, ms_e2e], dev)
     if rank != 0:
         return None
 
