@@ -71,3 +71,30 @@ def test_closed_form_on_small_widths():
             for r in range(0, 10):
                 for m in masks(nzb, rng, 6):
                     assert closed_form(m, zblk, nzb, r) == by_interval(m, zblk, r, width)
+
+
+def zwindow_mask(width, zblk, zl, zh):
+    """egg_stencil.cuh zwindow_mask: bits of the blocks meeting cells [zl, zh]."""
+    bl, bh = max(0, zl) // zblk, min(width - 1, zh) // zblk
+    return ((2 << bh) - (1 << bl)) & ((1 << 64) - 1)
+
+
+@pytest.mark.parametrize("n,d,eps", [(1_000_000, 3, 0.015), (20_000, 16, 0.15), (100_000, 5, 0.08), (45_781, 3, 0.05)])
+def test_column_mask_never_hides_a_candidate(n, d, eps):
+    """A column is passed over only when no cell of it lies in the lane's
+    window [z - r - 1, z + r + 1] (the range its two binary searches cover)."""
+    g = Oracle().geometry(n, d, eps)
+    if g.od >= d:
+        pytest.skip("no inner dimension")
+    zblk, nzb = blocks(g.width, g.od, d)
+    rng = np.random.default_rng(n)
+    for _ in range(300):
+        cells = np.unique(rng.integers(0, g.width, int(rng.integers(0, 12))))
+        colmask = 0
+        for z in cells:
+            colmask |= 1 << int(z // zblk)
+        z = int(rng.integers(0, g.width))
+        zl, zh = z - g.r - 1, z + g.r + 1
+        has = bool(((cells >= zl) & (cells <= zh)).any())
+        passes = (colmask & zwindow_mask(g.width, zblk, zl, zh)) != 0
+        assert passes or not has
