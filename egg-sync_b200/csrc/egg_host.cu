@@ -913,11 +913,14 @@ int grid_noalloc(const float* x, int64_t n, int32_t d, float eps, int32_t* order
         src = xin;
     }
     launch_transpose_in(g, w, src, st);
-    launch_build(single(g, w), st);
+    // non-finite input is rejected before the build runs on it (as egg_sync_grid does)
     int ctrl_h[kCtrlWords];
     EGG_CHECK(cudaMemcpyAsync(ctrl_h, w.ctrl, sizeof(ctrl_h), cudaMemcpyDeviceToHost, st));
     EGG_CHECK(cudaStreamSynchronize(st));
     if (ctrl_h[kCtrlStatus] & kErrNonFinite) throw ArgError{EGG_ERR_INPUT, "input holds NaN or Inf"};
+    launch_build(single(g, w), st);
+    EGG_CHECK(cudaMemcpyAsync(ctrl_h, w.ctrl, sizeof(ctrl_h), cudaMemcpyDeviceToHost, st));
+    EGG_CHECK(cudaStreamSynchronize(st));
     const int M = ctrl_h[kCtrlM];
     EGG_CHECK(cudaMemcpyAsync(order, w.orig, sizeof(int) * (size_t)g.n, cudaMemcpyDefault, st));
     EGG_CHECK(cudaMemcpyAsync(cell_of, w.cell_of, sizeof(int) * (size_t)g.n, cudaMemcpyDefault, st));
@@ -931,6 +934,9 @@ int grid_noalloc(const float* x, int64_t n, int32_t d, float eps, int32_t* order
 int release() {
     release_batch();
     mlp::release_all();
+    // a device reset after this call may place the static scratch elsewhere:
+    // the next allocation-free call looks its address up again
+    for (auto& p : g_noalloc_addr) p = nullptr;
     for (auto& kv : g_inst) {
         Instance* I = kv.second;
         int cur = 0;

@@ -161,7 +161,11 @@ int egg_sync_grid(const float *x, int64_t n, int32_t d, float eps, int32_t *orde
  * Limits: 1 <= n <= 65536 and 1 <= d <= 4; larger inputs return EGG_ERR_ARG.
  * The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture.  Every call reuses the same array and finds the
+ * before any stream capture.  egg_release() forgets the address, so the
+ * first call after it looks it up again: call egg_release() before a device
+ * reset (cudaDeviceReset), after which the array may sit elsewhere.  Input
+ * holding NaN or Inf returns EGG_ERR_INPUT before the build runs.  Every
+ * call reuses the same array and finds the
  * previous call's contents in it (the call clears what must start at zero);
  * two calls overlapping on the GPU would race on it.  Calls through this
  * library are serialised and each one has finished on the GPU before it

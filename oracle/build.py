@@ -2,8 +2,9 @@
 
 * ``build_oracle()`` compiles the C restatement ``oracle/egg_oracle.c`` into
   ``oracle/_build/libeggoracle.so``.
-* ``build_ref()`` compiles the reference's own sources, where they lie under
-  ``/root/reference`` (never copied), together with the two thin C-ABI
+* ``build_ref()`` compiles the reference's own sources, where they lie in
+  the reference tree (its location comes from the ``root`` argument or the
+  ``EGG_REFERENCE_ROOT`` environment variable; never copied), together with the two thin C-ABI
   drivers in this folder, into ``oracle/_ref/``:
 
   - ``libref_sync.so``: ``src/algorithms/SynC.cpp`` + ``src/utils/CPU_math.cpp``
@@ -29,7 +30,6 @@ import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REF_ROOT = Path(os.environ.get("EGG_REFERENCE_ROOT", "/root/reference"))
 BUILD_DIR = HERE / "_build"
 REF_DIR = HERE / "_ref"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -71,18 +71,26 @@ def _torch_flags():
     return inc, abi, link
 
 
-def ref_available() -> bool:
-    return (REF_ROOT / "src" / "algorithms" / "SynC.cpp").exists()
+def ref_root(root=None):
+    """The reference tree: ``root`` if given, else ``EGG_REFERENCE_ROOT``, else None."""
+    r = root if root is not None else os.environ.get("EGG_REFERENCE_ROOT")
+    return Path(r) if r else None
 
 
-def build_ref(force: bool = False, with_gpu: bool = True) -> dict:
+def ref_available(root=None) -> bool:
+    r = ref_root(root)
+    return r is not None and (r / "src" / "algorithms" / "SynC.cpp").exists()
+
+
+def build_ref(force: bool = False, with_gpu: bool = True, root=None) -> dict:
     """Compile the reference CPU SynC (and, with ``with_gpu``, EGG-SynC and the
-    brute-force GPU SynC)."""
-    if not ref_available():
-        raise FileNotFoundError("reference sources not found under %s" % REF_ROOT)
+    brute-force GPU SynC) from the reference tree ``root`` (default:
+    ``EGG_REFERENCE_ROOT``)."""
+    if not ref_available(root):
+        raise FileNotFoundError("reference sources not found (give root= or set EGG_REFERENCE_ROOT)")
     REF_DIR.mkdir(exist_ok=True)
     inc, abi, link = _torch_flags()
-    src = REF_ROOT / "src"
+    src = ref_root(root) / "src"
     out = {}
 
     sync_so = REF_DIR / "libref_sync.so"
@@ -140,6 +148,8 @@ def build_ref(force: bool = False, with_gpu: bool = True) -> dict:
 
 
 if __name__ == "__main__":
+    # python oracle/build.py [--force] [--no-gpu] [--ref REFERENCE_TREE]
     print(build_oracle(force="--force" in sys.argv))
-    if ref_available():
-        print(build_ref(force="--force" in sys.argv, with_gpu="--no-gpu" not in sys.argv))
+    root = sys.argv[sys.argv.index("--ref") + 1] if "--ref" in sys.argv else None
+    if ref_available(root):
+        print(build_ref(force="--force" in sys.argv, with_gpu="--no-gpu" not in sys.argv, root=root))

@@ -1,12 +1,12 @@
 """Golden vectors of the MDL eps search pieces from the reference's own code.
 
 Runs NN(k, D) and L_Clust_Outl(D, M) of python/SynCTorch.py (the reference
-tree must be present at REF) on small seeded inputs and writes
+tree is the first argument, or EGG_REFERENCE_ROOT) on small seeded inputs and writes
 tests/golden/ref_mdl.npz.  The reference module uses ``double('inf')``
 without defining ``double``; the generator supplies ``double = float``
 (the only change) so that NN runs as written.
 
-    python tests/golden/make_mdl_golden.py [REF]
+    python tests/golden/make_mdl_golden.py REFERENCE_TREE
 """
 import contextlib
 import importlib.util
@@ -19,7 +19,12 @@ import scipy.stats  # noqa: F401  (the reference reaches scipy.stats.iqr through
 import torch
 
 HERE = Path(__file__).resolve().parent
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+import os
+
+_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("EGG_REFERENCE_ROOT")
+if not _root:
+    sys.exit("usage: make_mdl_golden.py REFERENCE_TREE (or set EGG_REFERENCE_ROOT)")
+REF = Path(_root)
 
 
 def load_ref():

@@ -50,3 +50,47 @@ def test_noalloc_rejects_inputs_beyond_its_limit(eggsync_lib):
     assert b"65536" in L.egg_last_error()
     st, *_ = grid_noalloc(L, np.zeros((10, 5), np.float32), 0.05)
     assert st == _lib.EGG_ERR_ARG
+
+
+def test_noalloc_at_its_limit_with_device_input(eggsync_lib, gpu):
+    """n = 65,536 and d = 4, the largest layout the 8 MiB array holds, with
+    the points already in device memory (no staging copy); twice in a row,
+    and once more after egg_release(), which makes the call look the
+    array's address up again."""
+    import torch
+
+    L = eggsync_lib
+    rng = np.random.default_rng(11)
+    centres = rng.uniform(0.1, 0.9, (12, 4))
+    X = (centres[rng.integers(0, 12, 65536)] + rng.normal(0, 0.02, (65536, 4))).astype(np.float32)
+    X = data.min_max_normalize(X)
+    for eps, release in ((0.08, False), (0.05, False), (0.05, True)):
+        if release:
+            assert L.egg_release() == _lib.EGG_OK
+        Xd = torch.from_numpy(X).to(gpu)
+        order = torch.empty(65536, dtype=torch.int32, device=gpu)
+        cell_of = torch.empty(65536, dtype=torch.int32, device=gpu)
+        start = torch.empty(65537, dtype=torch.int32, device=gpu)
+        M = C.c_int32(0)
+        torch.cuda.synchronize()
+        st = L.egg_sync_grid_noalloc(C.c_void_p(Xd.data_ptr()), 65536, 4, eps, C.c_void_p(order.data_ptr()),
+                                     C.c_void_p(cell_of.data_ptr()), C.c_void_p(start.data_ptr()), C.byref(M), None)
+        assert st == _lib.EGG_OK, L.egg_last_error()
+        r_order, r_cell_of, r_start = egg_grid(X, eps)
+        assert np.array_equal(order.cpu().numpy(), r_order)
+        assert np.array_equal(cell_of.cpu().numpy(), r_cell_of)
+        assert np.array_equal(start.cpu().numpy()[: M.value + 1], r_start)
+
+
+def test_noalloc_rejects_non_finite_input(eggsync_lib):
+    L = eggsync_lib
+    X = np.random.default_rng(3).random((500, 3)).astype(np.float32)
+    X[17, 2] = np.inf
+    st, *_ = grid_noalloc(L, X, 0.05)
+    assert st == _lib.EGG_ERR_INPUT
+    # the next call on finite input works
+    X[17, 2] = 0.5
+    st, order, cell_of, start = grid_noalloc(L, X, 0.05)
+    assert st == _lib.EGG_OK
+    r_order, _, r_start = egg_grid(X, 0.05)
+    assert np.array_equal(order, r_order) and np.array_equal(start, r_start)
