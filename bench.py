@@ -49,9 +49,14 @@ sys.path.insert(0, str(REPO / "egg-sync_b200"))
 METRIC = "time-to-converged-labels (s) at 1M x 3D"
 WORKLOAD = "egg-sync plain loop, 1M x 3D, 50 Gaussian clusters + 10% noise, eps 0.015 (c5 shape, seed 0)"
 L2_FLUSH_BYTES = 256 << 20
-# Iterations the reference EGG semantics take on this workload (measured by
-# the plain GPU path; used only to extrapolate the CPU baseline).
-C5_ITERATIONS = 191
+# Iterations the reference CPU SynC takes on this workload: its lambda stop
+# rule (SynC.cpp:277) reached after 10 iterations, r_local 0.99933, counted
+# by `python bench.py --sync-iterations` (the brute-force GPU SynC follows
+# the same rule; 15 s on one B200).  Used only to extrapolate the CPU
+# baseline, whose full run would take hours.
+C5_SYNC_ITERATIONS = 10
+# points in the timed sample of the CPU baseline
+CPU_SAMPLE = 4000
 # DRAM bytes (read + written) of one update launch on this workload, mean over
 # the 191 launches of a run, from one ncu capture of the dram__bytes counters
 # (python bench.py --profile-run under ncu -k regex:k_update).
@@ -71,6 +76,12 @@ def parse():
     ap.add_argument("--profile-run", action="store_true",
                     help="for ncu: one warm-up run and one run of the workload through the host-driven loop, "
                          "no timing, no CPU baseline")
+    ap.add_argument("--sync-iterations", action="store_true",
+                    help="count the reference CPU SynC's iterations on the workload (brute-force GPU SynC)")
+    ap.add_argument("--sync-max-iter", type=int, default=300)
+    ap.add_argument("--profile-grid", action="store_true",
+                    help="for ncu: six grid builds of the workload from device-resident points (L2 flushed "
+                         "before each), no timing")
     return ap.parse_args()
 
 
@@ -89,6 +100,25 @@ def profile_run(args):
     torch.cuda.synchronize(dev)
     print(json.dumps({"profile_run": True, "n": len(c["X"]), "iterations": info["iterations"],
                       "launches_per_run": info["launches"]}))
+
+
+def profile_grid(args):
+    """Six builds of the double grid (egg_sync_grid) of the workload from
+    device-resident points, the L2 flushed before each: every grid/scan kernel
+    runs on a fresh input (no unchanged-grid early exit)."""
+    import torch
+
+    from eggsync import data, egg_grid
+
+    dev = torch.device("cuda", 0)
+    c = data.c5(args.seed, n=args.n)
+    Xd = torch.from_numpy(c["X"]).to(dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    for _ in range(6):
+        flush.zero_()
+        _, _, start = egg_grid(Xd, c["eps"])
+    torch.cuda.synchronize(dev)
+    print(json.dumps({"profile_grid": True, "n": len(c["X"]), "cells": len(start) - 1}))
 
 
 def dist_setup(args):
@@ -196,27 +226,54 @@ def update_bytes_per_launch(n, d, cells):
     return n * (4 * d + 8 * d + 4 * d) + cells * (4 + 4 * d + 8 * d)
 
 
-def cpu_baseline(X, eps, iterations, sample, seed=0):
-    """Reference CPU SynC (SynC.cpp:16-56, OpenMP) on `sample` points of one
-    iteration against all n points; extrapolated to n points x iterations."""
+def cpu_sample_idx(n, sample):
+    """The points whose reference CPU SynC iteration is timed: a fixed random
+    sample (seed 0), the same in the cpu_baseline leg and the reference arm."""
+    return np.sort(np.random.default_rng(0).choice(n, sample, replace=False)).astype(np.int32)
+
+
+def cpu_iteration_time(R, X, eps, sample):
+    """Seconds of one reference CPU SynC iteration over all n points,
+    estimated from `sample` points timed against all n (each point's work is
+    one pass over all n points: SynC.cpp:16-56)."""
+    idx = cpu_sample_idx(len(X), sample)
+    t0 = time.perf_counter()
+    R.step_sample(X, eps, idx)
+    dt = time.perf_counter() - t0
+    return dt / sample * len(X), dt
+
+
+def cpu_baseline(X, eps, sample, full_c1=True):
+    """Reference CPU SynC (SynC.cpp, OpenMP, all host threads): one iteration
+    over all n points estimated from a timed sample, times the CPU SynC's own
+    iteration count on this workload (an extrapolation: a full run is hours);
+    plus one measured full run to labels at 10,000 x 2D (eggsync.data.c1)."""
     sys.path.insert(0, str(REPO / "oracle"))
+    from eggsync import data
     from oracle import RefSync
 
     R = RefSync()
     n = len(X)
-    idx = np.random.default_rng(seed).choice(n, sample, replace=False).astype(np.int32)
-    t0 = time.perf_counter()
-    R.step_sample(X, eps, idx)
-    dt = time.perf_counter() - t0
-    per_point = dt / sample
-    return {
-        "value": per_point * n * iterations,
+    per_iter, dt = cpu_iteration_time(R, X, eps, sample)
+    out = {
+        "value": per_iter * C5_SYNC_ITERATIONS,
         "unit": "s",
         "cores": R.threads(),
         "kind": "reference",
-        "sample": "reference SynC parallel (OpenMP) one iteration for %d of %d points against all %d, %.2f s; "
-                  "extrapolated x%d points x %d iterations (EGG iteration count)" % (sample, n, n, dt, n, iterations),
+        "sample": "reference SynC parallel (OpenMP): one iteration of %d sampled points (seed 0) against all %d, "
+                  "%.2f s -> %.1f s per full iteration; extrapolated x %d iterations, the CPU SynC's own count on "
+                  "this workload (lambda stop rule, counted with the brute-force GPU SynC, bench.py "
+                  "--sync-iterations)" % (sample, n, dt, per_iter, C5_SYNC_ITERATIONS),
+        "s_per_iteration": per_iter,
+        "extrapolated": True,
     }
+    if full_c1:
+        c = data.c1(0)
+        t0 = time.perf_counter()
+        _, it = R.run(c["X"], c["eps"], c["lam"])
+        out["measured_c1"] = {"workload": "10,000 x 2D, eps 0.05, lambda 1-1e-3 (c1, seed 0)",
+                              "time_to_labels_s": time.perf_counter() - t0, "iterations": it}
+    return out
 
 
 def run_ours(args, rank, local, world, pg):
@@ -286,7 +343,7 @@ def run_ours(args, rank, local, world, pg):
     ub = update_bytes_per_launch(n, d, cells)
     achieved = ub / (upd_ms * 1e-3) / 1e9
     tot_k = sum(pinfo["kernel_ms"].values())
-    sample = args.cpu_sample or 2000
+    sample = args.cpu_sample or CPU_SAMPLE
     line = {
         "metric": METRIC,
         "value": t_max / 1000.0,
@@ -317,7 +374,7 @@ def run_ours(args, rank, local, world, pg):
         "kernel_ms": pinfo["kernel_ms"],
         "stage_ms": info["stage_ms"],
         "clocks": clocks,
-        "cpu_baseline": cpu_baseline(X, eps, iters, sample),
+        "cpu_baseline": cpu_baseline(X, eps, sample),
     }
     if learned is not None:
         line["learned"] = learned
@@ -447,22 +504,33 @@ def mdl_leg(dev):
 
 
 def run_reference(args, rank, world):
+    """The reference's own CPU SynC on the box's host cores (rank 0 only):
+    every step times one iteration of the same fixed sample as the
+    cpu_baseline leg and extrapolates to the whole run."""
     if rank != 0:
         return None
     sys.path.insert(0, str(REPO / "oracle"))
     from eggsync import data
+    from oracle import RefSync
 
     c = data.c5(args.seed, n=args.n)
     X, eps = c["X"], c["eps"]
-    iters = C5_ITERATIONS or 1
-    sample = args.cpu_sample or 400
+    sample = args.cpu_sample or CPU_SAMPLE
+    R = RefSync()
     vals = []
+    dts = []
     for k in range(args.warmup + args.steps):
-        cb = cpu_baseline(X, eps, iters, sample, seed=k)
+        per_iter, dt = cpu_iteration_time(R, X, eps, sample)
         if k >= args.warmup:
-            vals.append(cb["value"])
+            vals.append(per_iter * C5_SYNC_ITERATIONS)
+            dts.append(dt)
     v = statistics.mean(vals)
+    cb = cpu_baseline(X, eps, sample)
     cb["value"] = v
+    cb["sample"] = ("reference SynC parallel (OpenMP): per step one iteration of %d sampled points (seed 0) against "
+                    "all %d, mean %.2f s over %d steps; extrapolated x n/sample x %d iterations (the CPU SynC's own "
+                    "count on this workload)" % (sample, len(X), statistics.mean(dts), args.steps,
+                                                 C5_SYNC_ITERATIONS))
     n, d = X.shape
     return {
         "metric": METRIC, "value": v, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -474,10 +542,34 @@ def run_reference(args, rank, world):
     }
 
 
+def sync_iterations(args):
+    """Iterations the reference CPU SynC (SynC.cpp:268-326: lambda stop rule
+    on the mean local order parameter, exact eps neighbourhoods) takes on the
+    workload, counted with this library's brute-force GPU SynC, which follows
+    the same rule (egg_simple_sync_run)."""
+    import torch
+
+    from eggsync import data, simple_sync
+
+    dev = torch.device("cuda", 0)
+    c = data.c5(args.seed, n=args.n)
+    Xd = torch.from_numpy(c["X"]).to(dev)
+    t0 = time.perf_counter()
+    lab, info = simple_sync(Xd, c["eps"], c["lam"], max_iter=args.sync_max_iter)
+    print(json.dumps({"sync_iterations": info["iterations"], "converged": info["converged"],
+                      "r_local": info["r_local"], "s": time.perf_counter() - t0, "n": len(c["X"])}))
+
+
 def main():
     args = parse()
     if args.profile_run:
         profile_run(args)
+        return
+    if args.profile_grid:
+        profile_grid(args)
+        return
+    if args.sync_iterations:
+        sync_iterations(args)
         return
     rank, local, world, pg = dist_setup(args)
     try:

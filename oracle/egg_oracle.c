@@ -554,6 +554,92 @@ ORACLE_API int egg_oracle_extra_check(const float *X, int n, int d, float eps, i
     return ok;
 }
 
+/* Number of (p, q) pairs the reference's extra check lists on X: the counter
+ * of kernel_float_grid_extra_check_part1_count (EGG_SynC.cu:767-878), i.e.
+ * for every p, over the cells of its eps_extra stencil that pass the small
+ * box test against eps_extra and are not fully inside eps (EGG_SynC.cu:
+ * 848-866), the points q with eps < |p - q| <= eps_extra (EGG_SynC.cu:
+ * 870-878).  The reference sizes its pair list from this count with int
+ * arithmetic (EGG_SynC.cu:878, 1010, 1449-1450), so it must stay below
+ * 2^30 and below n*n mod 2^32 (the wrap limit of its atomicInc).
+ * Cells are decided wholesale by the tight box of their points where that
+ * box proves all or none of their points lie in the (eps, eps_extra]
+ * annulus; only straddling cells are walked.  *max_per_point (optional)
+ * receives the largest count of a single p. */
+ORACLE_API int64_t egg_oracle_ref_annulus_pairs(const float *X, int n, int d, float eps, int64_t *max_per_point) {
+    grid_t G;
+    if (d > 64 || grid_build(&G, X, n, d, eps) != 0) return -1;
+    float *lo = (float *)malloc(sizeof(float) * (size_t)G.M * d);
+    float *hi = (float *)malloc(sizeof(float) * (size_t)G.M * d);
+    for (int c = 0; c < G.M; c++) {
+        for (int l = 0; l < d; l++) { lo[(size_t)c * d + l] = FLT_MAX; hi[(size_t)c * d + l] = -FLT_MAX; }
+        for (int i = G.cell_start[c]; i < G.cell_start[c + 1]; i++) {
+            const float *xq = &X[(size_t)G.order[i] * d];
+            for (int l = 0; l < d; l++) {
+                if (xq[l] < lo[(size_t)c * d + l]) lo[(size_t)c * d + l] = xq[l];
+                if (xq[l] > hi[(size_t)c * d + l]) hi[(size_t)c * d + l] = xq[l];
+            }
+        }
+    }
+    int64_t total = 0, worst = 0;
+    const egg_geom *g = &G.g;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : total) reduction(max : worst)
+    for (int p = 0; p < n; p++) {
+        const float *xp = &X[(size_t)p * d];
+        const int *gp = &G.gid[(size_t)p * d];
+        const int od = g->od, W = g->width, rad = g->r_extra;
+        int idx[64];
+        int64_t mine = 0;
+        for (int l = 0; l < od; l++) idx[l] = -rad;
+        for (;;) {
+            int ok = 1;
+            int64_t o = 0, mul = 1;
+            for (int l = 0; l < od; l++) {
+                int v = gp[l] + idx[l];
+                if (v < 0 || v >= W) { ok = 0; break; }
+                o += (int64_t)v * mul; mul *= W;
+            }
+            if (ok) {
+                for (int c = G.outer_begin[o]; c < G.outer_begin[o + 1]; c++) {
+                    float sm2, lg2;
+                    box_dist2(xp, &G.cell_dims[(size_t)c * d], d, g, &sm2, &lg2);
+                    if (!(sm2 <= g->t_extra) || lg2 <= g->t_eps) continue;
+                    float n2 = 0.f, f2 = 0.f;
+                    for (int l = 0; l < d; l++) {
+                        const float L = lo[(size_t)c * d + l], H = hi[(size_t)c * d + l];
+                        float a = xp[l] < L ? L - xp[l] : (xp[l] > H ? xp[l] - H : 0.0f);
+                        float b1 = fabsf(L - xp[l]), b2 = fabsf(H - xp[l]);
+                        float b = b1 > b2 ? b1 : b2;
+                        n2 = fmaf(a, a, n2);
+                        f2 = fmaf(b, b, f2);
+                    }
+                    if (n2 > g->t_extra || f2 <= g->t_eps) continue;
+                    if (n2 > g->t_eps && f2 <= g->t_extra) {
+                        mine += G.cell_start[c + 1] - G.cell_start[c];
+                        continue;
+                    }
+                    for (int i = G.cell_start[c]; i < G.cell_start[c + 1]; i++) {
+                        float d2 = pdist2(xp, &X[(size_t)G.order[i] * d], d);
+                        mine += (d2 > g->t_eps && d2 <= g->t_extra);
+                    }
+                }
+            }
+            if (od == 0) break;
+            int l = 0;
+            idx[0]++;
+            while (l < od - 1 && idx[l] > rad) { idx[l] = -rad; l++; idx[l]++; }
+            if (idx[od - 1] > rad) break;
+        }
+        total += mine;
+        if (mine > worst) worst = mine;
+    }
+    free(lo);
+    free(hi);
+    grid_free(&G);
+    if (max_per_point) *max_per_point = worst;
+    return total;
+}
+
 /* -------------------------------- labels -------------------------------- */
 /* GPU_synCluster_float_grid, EGG_SynC.cu:1205-1227: label = compacted cell
  * index when the cell holds more than one point, else -1.  Cells are ranked

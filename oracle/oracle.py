@@ -73,6 +73,8 @@ class Oracle:
         L.egg_oracle_threads.restype = C.c_int
         L.egg_oracle_step_sample.argtypes = [_f32p, C.c_int, C.c_int, C.c_float, _i32p, C.c_int, _f32p, _i32p,
                                              _i32p]
+        L.egg_oracle_ref_annulus_pairs.argtypes = [_f32p, C.c_int, C.c_int, C.c_float, C.POINTER(C.c_int64)]
+        L.egg_oracle_ref_annulus_pairs.restype = C.c_int64
         L.egg_oracle_set_box_mode.argtypes = [C.c_int]
         L.egg_oracle_set_box_mode.restype = None
         L.egg_oracle_set_face_fma.argtypes = [C.c_int]
@@ -128,6 +130,14 @@ class Oracle:
         pairs = C.c_int64(0)
         ok = self.L.egg_oracle_extra_check(X, X.shape[0], X.shape[1], float(eps), C.byref(pairs))
         return ok, pairs.value
+
+    def ref_annulus_pairs(self, X, eps):
+        """(total, largest per point) of the pairs the reference's extra check
+        lists on X (EGG_SynC.cu:767-878)."""
+        X = _as_x(X)
+        worst = C.c_int64(0)
+        total = self.L.egg_oracle_ref_annulus_pairs(X, X.shape[0], X.shape[1], float(eps), C.byref(worst))
+        return int(total), int(worst.value)
 
     def labels(self, X, eps):
         X = _as_x(X)
@@ -218,8 +228,10 @@ class RefSync:
 
 
 _REF_EGG_CHILD = r"""
-import sys, json, ctypes as C, numpy as np, torch
+import sys, json, time, ctypes as C, numpy as np, torch
 X = np.load(sys.argv[2]).astype(np.float32)
+if torch.cuda.is_available():
+    torch.zeros(1, device="cuda")  # the CUDA context exists before the timed call
 eps = float(sys.argv[3])
 L = C.CDLL(sys.argv[1])
 n, d = X.shape
@@ -229,27 +241,47 @@ st = np.zeros(6, np.float32)
 f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 L.ref_egg_run.argtypes = [f32p, C.c_int, C.c_int, C.c_float, i32p, C.POINTER(C.c_int), f32p]
-rc = L.ref_egg_run(np.ascontiguousarray(X), n, d, eps, lab, C.byref(it), st)
+Xc = np.ascontiguousarray(X)
+t0 = time.perf_counter()
+rc = L.ref_egg_run(Xc, n, d, eps, lab, C.byref(it), st)
+wall = time.perf_counter() - t0
 np.save(sys.argv[4], lab)
-sys.stderr.write("REF_EGG_RESULT " + json.dumps({"rc": rc, "iters": it.value, "stage_times": st.tolist()}) + "\n")
+sys.stderr.write("REF_EGG_RESULT " + json.dumps({"rc": rc, "iters": it.value, "stage_times": st.tolist(),
+                                                 "wall_s": wall}) + "\n")
 """
 
-# The reference EGG-SynC's extra check sizes its pair list with an int and an
-# atomicInc limit of n*n (EGG_SynC.cu:878, 1010, 1449-1450); both stay inside
-# int range only while 2*n*n < 2^31, i.e. n <= 32768.  It is only ever run on
-# such inputs.
+# The reference EGG-SynC's extra check counts its pairs with
+# atomicInc(counter, n * n) and sizes its pair list with int arithmetic
+# (EGG_SynC.cu:878, 1010, 1449-1450): the int product n * n wraps (mod 2^32,
+# read as unsigned by atomicInc, which restarts at 0 past that limit), and
+# 2 * count must fit in an int.  For n <= 32768 every possible count is
+# inside both limits; above it the reference is defined only while the
+# counts of the iterations that run the extra check stay below
+# ref_egg_pair_limit(n) (counted with Oracle.ref_annulus_pairs first).
 REF_EGG_MAX_N = 32768
 
 
-def run_ref_egg(X, eps, timeout=600, workdir=None):
+def ref_egg_pair_limit(n):
+    """Largest number of extra-check pairs + 1 the reference handles at n points."""
+    wrap = (n * n) % (1 << 32)
+    return min(1 << 30, wrap)
+
+
+def run_ref_egg(X, eps, timeout=600, workdir=None, max_pairs=None, info_out=None):
     """Run the reference EGG-SynC on X in a child process.
+
+    For n > 32768 the caller passes ``max_pairs``, the largest pair count of
+    the reference's extra check over the run (counted beforehand); the run
+    is refused unless it is below ``ref_egg_pair_limit(n)``.  ``info_out``
+    (a dict) receives the child's wall time of the call.
 
     Returns (labels, iterations, stage_times)."""
     import tempfile
 
     X = _as_x(X)
-    if X.shape[0] > REF_EGG_MAX_N:
-        raise ValueError("reference EGG-SynC is only run for n <= %d" % REF_EGG_MAX_N)
+    if X.shape[0] > REF_EGG_MAX_N and (max_pairs is None or max_pairs >= ref_egg_pair_limit(X.shape[0])):
+        raise ValueError("reference EGG-SynC at n = %d needs a pair count below %d (got %s)" %
+                         (X.shape[0], ref_egg_pair_limit(X.shape[0]), max_pairs))
     so = _build.REF_DIR / "libref_egg.so"
     if not so.exists():
         raise FileNotFoundError(str(so))
@@ -265,6 +297,8 @@ def run_ref_egg(X, eps, timeout=600, workdir=None):
                 info = json.loads(line[len("REF_EGG_RESULT "):])
         if r.returncode != 0 or info is None or info["rc"] != 0:
             raise RuntimeError("reference EGG-SynC failed (rc=%s): %s" % (r.returncode, r.stderr[-2000:]))
+        if info_out is not None:
+            info_out.update(info)
         return np.load(lout), info["iters"], info["stage_times"]
 
 

@@ -161,3 +161,47 @@ def test_extra_check_detects_pull(oracle):
     # without r the MBR of q is q itself, outside eps: converged
     ok2, pairs2 = oracle.extra_check(np.stack([p, q]), eps)
     assert pairs2 >= 1 and ok2 == 1
+
+
+def test_ref_annulus_pairs_equals_walked_count(oracle):
+    """The reference's extra-check pair count (EGG_SynC.cu:767-878), counted
+    with tight-box shortcuts, equals the count of the oracle's plain walk
+    over the same cells on converged input (no veto, so every pair is
+    walked), and the 2-D layout of five tight clusters 0.051 apart (inside
+    the (eps, eps_extra] annulus of their neighbours) bounds it."""
+    rng = np.random.default_rng(5)
+    eps = np.float32(0.05)
+    X = np.concatenate([np.array([0.2 + 0.051 * k, 0.5]) + rng.uniform(-1e-4, 1e-4, (40, 2)) for k in range(5)])
+    X = X.astype(np.float32)
+    ok, walked = oracle.extra_check(X, eps)
+    total, worst = oracle.ref_annulus_pairs(X, eps)
+    assert ok == 1
+    assert total == walked
+    assert 0 < total <= 2 * 4 * 40 * 40
+    assert 0 < worst <= 80
+
+
+@pytest.mark.parametrize("name", ["c3b_s0", "c2_s0", "c5_s0"])
+def test_large_reference_fixtures(name):
+    """The reference EGG-SynC fixtures of the large workloads: made from the
+    same inputs, the reference's pair count stayed inside its int limits, and
+    its repeated runs gave one partition and one iteration count."""
+    from make_golden import checksum
+    from oracle import ref_egg_pair_limit
+
+    G = load_golden("ref_egg_%s.npz" % name)
+    X = {"c3b_s0": data.c3b, "c2_s0": data.c2, "c5_s0": data.c5}[name](0)["X"]
+    assert checksum(X) == G["x_checksum"]
+    assert int(G["ref_ran"]) == 1 and int(G["ref_runs_same_partition"]) == 1
+    assert G["pair_rows"][:, 1].max() < ref_egg_pair_limit(len(X)) == int(G["pair_limit"])
+    assert len(set(G["iterations"].tolist())) == 1
+    assert G["labels"].shape == (1, len(X))
+
+
+def test_disputed_points_counts_only_the_minority():
+    from test_gpu_large import disputed_points
+
+    a = np.array([0, 0, 0, 1, 1, 1, -1, -1], np.int32)
+    b = np.array([5, 5, 7, 2, 2, 2, -1, 3], np.int32)
+    assert disputed_points(a, b).tolist() == [2, 7]
+    assert len(disputed_points(a, a)) == 0
