@@ -226,6 +226,108 @@ def update_bytes_per_launch(n, d, cells):
     return n * (4 * d + 8 * d + 4 * d) + cells * (4 + 4 * d + 8 * d)
 
 
+def grid_bytes(n, d, width, cells, n_outer):
+    """Algorithmic bytes of one full grid build from device-resident points
+    (egg_sync_grid, the grid of EGG_SynC.cu:248-341): the input transpose
+    (row-major read, per-dimension write, original index), the grid check's
+    copy, per radix pass the digit reads through the permutation (all d
+    coordinates in the first, sub-cell pass; one per later pass) and the
+    permutation read/write, the tile histograms, the gather into sorted
+    order, the cell heads and records, the outer ranges."""
+    digits = 1 if width <= 256 else 2
+    passes = 1 + d * digits
+    tiles = (n + 4095) // 4096
+    per_point = (4 * d + 4 * d + 4)          # transpose
+    per_point += 8 * d                       # grid check: read Xn, write X
+    per_point += 4 * d + 4 * d + 4           # sub-cell pass: hist + scatter (first pass reads no permutation)
+    per_point += (passes - 1) * (8 + 12)     # later passes: hist (perm + digit), scatter (perm + digit + perm out)
+    per_point += 4 + 4 * d + 4 + 4 * d + 4   # gather: perm, Xn, orig in; X, orig_tmp out
+    per_point += 4 * d + 4 + 4 + 4           # heads: X, orig_tmp in; cell_of, orig out
+    hist = passes * tiles * 256 * 4 * 4      # histogram write, scan read + write, scatter read
+    return n * per_point + cells * (4 + 4 * d + 4 + 8) + (n_outer + 1) * 12 + hist
+
+
+def grid_leg(Xd, eps, dev, flush, reps=10):
+    """The grid build (egg_sync_grid, device input and outputs) timed with
+    CUDA events on the calling stream, the L2 flushed before each build;
+    against the measured HBM bandwidth."""
+    import torch
+
+    from eggsync import egg_grid
+
+    n, d = Xd.shape
+    out = (torch.empty(n, dtype=torch.int32, device=dev), torch.empty(n, dtype=torch.int32, device=dev),
+           torch.empty(n + 1, dtype=torch.int32, device=dev))
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(3):
+        _, _, start = egg_grid(Xd, eps, out=out)
+    times = []
+    for _ in range(reps):
+        flush.zero_()
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        _, _, start = egg_grid(Xd, eps, out=out)
+        e.record(stream)
+        e.synchronize()
+        times.append(s.elapsed_time(e))
+    ms = statistics.median(times)
+    side = float(np.float32(np.sqrt((eps / 2) ** 2 / d)))
+    width = int(np.float32(1.0) / np.float32(side))
+    od = min(d, int(np.log(n) / np.log(width)))
+    b = grid_bytes(n, d, width, len(start) - 1, width ** od)
+    peak, kind = measured_peaks()
+    ach = b / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": "grid build (egg_sync_grid: transpose, check, radix passes, heads, outer ranges)",
+            "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_source": kind,
+            "ms_per_build": ms, "algorithmic_bytes": b, "cells": len(start) - 1,
+            "note": "the timed call includes the entry point's two host synchronisations and its output copies "
+                    "(order, cell_of, cell_start); per-kernel DRAM bytes and times: profiles/grid_scan_c5_1M.md"}
+
+
+_STATS_CHILD = r"""
+import ctypes as C, json, os, sys
+sys.path.insert(0, sys.argv[1])
+from eggsync import _lib, data, egg_sync
+c = data.c5(int(sys.argv[2]), n=int(sys.argv[3]))
+egg_sync(c["X"], c["eps"])
+out = (C.c_int64 * 64)()
+k = _lib.load().egg_update_counters(out, 64)
+print(json.dumps(dict(zip(_lib.UPDATE_COUNTERS, [int(v) for v in out[:k]]))))
+"""
+
+
+def update_fp32_leg(args, update_ms):
+    """Algorithmic FP32 work of the update kernel over one run, from the
+    interaction counters of the stats build (libeggsync_stats.so, same
+    results), over the update kernel's CUDA-event time of the profiled run,
+    against the nominal FP32 rate of the chip (148 SMs x 128 lanes x 2 flops
+    x the measured SM clock).  Flops counted: the reference's box test per
+    visited cell (3 per dimension: two fused face offsets and a square), the
+    tight-box test per passing cell, 6 per dimension per aggregated cell or
+    group (the frame change), 3 per dimension per point-pair distance test
+    and 2 per dimension per counted pair."""
+    lib = REPO / "egg-sync_b200" / "lib" / "libeggsync_stats.so"
+    if not lib.exists():
+        return None
+    env = dict(os.environ, EGGSYNC_LIB=str(lib))
+    r = subprocess.run([sys.executable, "-c", _STATS_CHILD, str(REPO / "egg-sync_b200"), str(args.seed), str(args.n)],
+                       env=env, capture_output=True, text=True, timeout=600)
+    if r.returncode != 0:
+        return {"error": r.stderr[-500:]}
+    k = json.loads(r.stdout.strip().splitlines()[-1])
+    d = 3
+    flops = (3 * d * k["cells"] + 3 * d * k["small_pass"] +
+             6 * d * (k["full"] + k["tight_in"] + k["groups_in"]) + 3 * d * k["pairs"] + 2 * d * k["pairs_in"])
+    ach = flops / (update_ms * 1e-3) / 1e12
+    peak = 148 * 128 * 2 * 1.965e9 / 1e12
+    return {"bound": "fp32", "kernel": "k_update", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+            "frac": ach / peak, "peak_source": "nominal (148 SMs x 128 FP32 lanes x 2 x 1965 MHz)",
+            "algorithmic_flops": flops, "counters": k,
+            "note": "issue-bound, not FP32-bound: warp-issue and lane-activity figures from ncu in "
+                    "profiles/k_update_c5_1M.md"}
+
+
 def cpu_sample_idx(n, sample):
     """The points whose reference CPU SynC iteration is timed: a fixed random
     sample (seed 0), the same in the cpu_baseline leg and the reference arm."""
@@ -325,6 +427,7 @@ def run_ours(args, rank, local, world, pg):
 
     # profiled run: every kernel group bracketed by CUDA events on its stream
     _, pinfo = egg_sync(Xd, eps, labels_out=lab_d, profile=True)
+    grid = grid_leg(Xd, eps, dev, flush) if world == 1 else None
     learned = learned_leg(args, timed, Xd, eps, lab_d, dev) if world == 1 and not args.no_extra else None
     sweep = batched_sweep(dev) if world == 1 and not args.no_extra else None
     mdl = mdl_leg(dev) if world == 1 and not args.no_extra else None
@@ -376,6 +479,9 @@ def run_ours(args, rank, local, world, pg):
         "clocks": clocks,
         "cpu_baseline": cpu_baseline(X, eps, sample),
     }
+    if grid is not None:
+        line["roofline_grid"] = grid
+        line["roofline_update_fp32"] = update_fp32_leg(args, pinfo["kernel_ms"]["update"])
     if learned is not None:
         line["learned"] = learned
     if sweep is not None:
@@ -453,10 +559,15 @@ def batched_sweep(dev):
     sres = [egg_sync(x, e, labels_out=o) for (x, e), o in zip(inst, os_)]
     torch.cuda.synchronize(dev)
     ts = time.perf_counter() - t0
+    # device time of the sequential calls (each call's CUDA events from its
+    # first to its last operation); the rest of the wall clock is host work:
+    # capturing and instantiating each call's loop graph, launches, syncs
+    seq_dev = sum(q[1]["total_ms"] for q in sres) / 1000.0
     same = all(torch.equal(a, b) for a, b in zip(ob, os_)) and all(
         r[1]["iterations"] == q[1]["iterations"] for r, q in zip(res, sres))
     return {"workload": "c4: 64 datasets (n 1k-200k, d in {2,3,5}) x 8 eps in [0.01, 0.08], 512 runs",
             "batched_s": min(tb), "sequential_s": ts, "speedup": ts / min(tb), "identical_to_sequential": same,
+            "sequential_device_s": seq_dev, "sequential_host_s": ts - seq_dev,
             "loop_iterations": bi["loop_iterations"], "launch_config": {k: bi[k] for k in (
                 "update_threads", "blocks_per_sm", "order")}}
 

@@ -676,7 +676,7 @@ void make_plan(State& S, Plan& P, egg_batch_item* items, int count, const egg_op
         S.base = nullptr;
         S.cap = 0;
         const size_t want = total + total / 8;
-        EGG_CHECK(cudaMalloc(&S.base, want));
+        EGG_CHECK(dev_alloc((void**)&S.base, want));
         S.cap = want;
     }
     char* b = (char*)S.base;

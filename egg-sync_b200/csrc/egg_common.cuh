@@ -16,7 +16,7 @@ namespace egg {
 
 constexpr int kMaxDims = 64;        // generic kernels support d <= kMaxDims
 constexpr int kMaxTable = 64;       // sin/cos table half-width: |k| <= kMaxTable
-constexpr int kSortTile = 4096;     // points per radix-sort tile
+constexpr int kSortTile = 2048;     // points per radix-sort tile (2048: 489 blocks at 1M points, 3.3 per SM)
 constexpr int kSortThreads = 256;
 constexpr int kHeadsBlock = 1024;   // points per block in the cell-boundary scan
 
@@ -175,7 +175,11 @@ enum : int {
     kUsNeighbors,      // sum of |N(p)|
     kUsCyclesShared,   // SM cycles of the candidate walk, warps whose lanes share one outer cell
     kUsCyclesLane,     // SM cycles of the candidate walk, warps whose lanes span several outer cells
-    kUStats = 16
+    kUsWarpVisits,     // candidate cells visited by lockstep warps (once per warp)
+    kUsCyclesVisits,   // SM cycles of those visits (box tests, aggregates, walks): the rest of
+                       // cycles_shared is the stencil enumeration
+    kUsWalkSteps,      // warp steps of the point walks (one per loop iteration a warp executes)
+    kUStats = 20
 };
 
 // ------------------------------------------------------------------------

@@ -97,10 +97,10 @@ __device__ bool mbr_exact(const Geom& g, const Work& w, int qi, const float* xp)
 
 // extremes of each point's eps/2 group (itself included)
 template <int D>
-__device__ __forceinline__ void ball_bbox_body(const Geom& g, const Work& w, int bx, int gx) {
+__device__ __forceinline__ void ball_bbox_body(const Geom& g, const Work& w, int bx, int gx, int mark = 1) {
     constexpr int DM = D > 0 ? D : kMaxDims;
     const int d = D > 0 ? D : g.d;
-    if (bx == 0 && threadIdx.x == 0) {
+    if (mark && bx == 0 && threadIdx.x == 0) {
         const int it = w.ctrl[kCtrlIter];
         w.stamps[4 * it + 2] = globaltimer();
         // the extra check runs in this iteration when the flag reached it
@@ -236,7 +236,9 @@ __device__ __forceinline__ void annulus_body(const Geom& g, const Work& w, int b
 }
 
 template <int D>
-__global__ void __launch_bounds__(128) k_ball_bbox(Geom g, Work w) { ball_bbox_body<D>(g, w, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(128) k_ball_bbox(Geom g, Work w, int mark) {
+    ball_bbox_body<D>(g, w, blockIdx.x, gridDim.x, mark);
+}
 template <int D>
 __global__ void __launch_bounds__(128) kb_ball_bbox(BatchArgs B) {
     batch_for(B, [&](const Geom& g, const Work& w, int bx, int gx) { ball_bbox_body<D>(g, w, bx, gx); });
@@ -265,9 +267,25 @@ __global__ void __launch_bounds__(128) kb_annulus(BatchArgs B) {
         default: KERNEL<0> __VA_ARGS__; break;        \
     }
 
-// Both kernels return at once unless the update left the flag at 1; the
-// grids are bounded so that the common early exit costs little.
-void launch_extra_check(const Exec& ex, cudaStream_t st) {
+// Opens the conditional node holding the extra check when the update left
+// the flag at 1 (the loop graph of a single instance), with the stage stamp
+// and the run count the first extra-check kernel keeps otherwise.
+__global__ void k_gate_extra(Work w, cudaGraphConditionalHandle h) {
+    const int it = w.ctrl[kCtrlIter];
+    w.stamps[4 * it + 2] = globaltimer();
+    const int flag = w.ctrl[kCtrlFlag];
+    if (flag != 0) atomicAdd(w.ctrl + kCtrlExtraRuns, 1);
+    cudaGraphSetConditional(h, flag != 0 ? 1u : 0u);
+}
+
+void launch_gate_extra(const Work& w, cudaGraphConditionalHandle h, cudaStream_t st) {
+    k_gate_extra<<<1, 1, 0, st>>>(w, h);
+}
+
+// The kernels return at once unless the update left the flag at 1; the
+// grids are bounded so that the common early exit costs little.  gated: the
+// call sits behind k_gate_extra, which did the stage stamp and the count.
+void launch_extra_check(const Exec& ex, cudaStream_t st, bool gated) {
     const int blocks = ex.blocks(kShapeCapN128, 128);
     if (ex.batch()) {
         const BatchArgs B = ex.args(kShapeCapN128);
@@ -275,7 +293,7 @@ void launch_extra_check(const Exec& ex, cudaStream_t st) {
         kb_cell_ballbox<<<ex.blocks(kShapeCapN128, 256), 256, 0, st>>>(B);
         EGG_DISPATCH_D(ex.d, kb_annulus, <<<blocks, 128, 0, st>>>(B));
     } else {
-        EGG_DISPATCH_D(ex.d, k_ball_bbox, <<<blocks, 128, 0, st>>>(*ex.g, *ex.w));
+        EGG_DISPATCH_D(ex.d, k_ball_bbox, <<<blocks, 128, 0, st>>>(*ex.g, *ex.w, gated ? 0 : 1));
         k_cell_ballbox<<<blocks, 256, 0, st>>>(*ex.g, *ex.w);
         EGG_DISPATCH_D(ex.d, k_annulus, <<<blocks, 128, 0, st>>>(*ex.g, *ex.w));
     }

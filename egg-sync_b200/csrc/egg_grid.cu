@@ -116,7 +116,9 @@ __device__ __forceinline__ size_t wp_idx(int field, int l, int d, int rec, int n
 // has any point left its cell?  A stable sort of unchanged keys is the
 // identity, so when no point changed cell the previous grid (order, cells,
 // outer ranges) is exactly the grid a rebuild would produce and every build
-// kernel below returns at once.  Also copies the positions into X.
+// kernel below returns at once.  Also copies the positions into X (with a
+// valid grid only for the warps the last update marked as moved: the
+// others hold Xn == X already).
 // ---------------------------------------------------------------------------
 template <int D>
 __device__ __forceinline__ void check_cells_body(const Geom& g, const Work& w, int bx, int gx) {
@@ -127,6 +129,10 @@ __device__ __forceinline__ void check_cells_body(const Geom& g, const Work& w, i
     constexpr bool kKeyed = D >= 1 && D <= 4;
     const bool keyed = kKeyed && w.cell_key != nullptr;
     for (int i = bx * blockDim.x + threadIdx.x; i < g.n; i += gx * blockDim.x) {
+        // with a valid grid, only the warps whose points the last update
+        // moved (it marks them) can differ from X: the others are skipped
+        // (blockDim is a multiple of 32, so the test is warp-uniform)
+        if (valid && w.warp_moved && w.warp_moved[i >> 5] == 0) continue;
         const int c = valid ? w.cell_of[i] : 0;
         bool moved = false;
         unsigned long long key = 0;

@@ -34,6 +34,7 @@ namespace egg {
 
 std::mutex g_mutex;
 thread_local std::string g_last_error;
+int g_fail_allocs = 0;  // injected allocation failures still to deliver (egg_inject_alloc_failures)
 // interaction counters of the last run (stats build)
 unsigned long long g_counters[kUStats] = {};
 
@@ -211,9 +212,40 @@ size_t layout_work(const Geom& g, int max_iter, char* base, Work& w, float** xin
     return off;
 }
 
+// The update stencil keeps only the outer columns that can hold a cell
+// passing the reference's small box test (EGG_SynC.cu:613-636).  For a cell
+// at offset k from the point's own cell, the nearer face in dimension l is
+// at least (|k_l| - 1) cells away (the point lies inside its own cell), so
+// the test sum_l min(left_l^2, right_l^2) <= eps^2 needs
+// sum_{l < od} ((|k_l| - 1)+)^2 <= eps^2 / side^2 (the other dimensions add
+// terms >= 0).  The bound is applied with a 1e-3 margin in cells and in the
+// squared radius, far above the float rounding of the cell ids and of the
+// test, so every cell the test can pass stays a candidate: the results do
+// not change, the corner columns are not visited.  (For d = 3 this drops 12
+// of the 81 columns of r = 4.)
+static Stencil screen_update_stencil(const Geom& g, const Stencil& full) {
+    const int od = g.od;
+    if (od == 0) return full;
+    Stencil S;
+    const double R2 = (double)g.t_eps / ((double)g.side * (double)g.side) * (1.0 + 1e-3);
+    auto excess = [](int k) {
+        const double v = std::abs(k) - 1.001;
+        return v > 0.0 ? v * v : 0.0;
+    };
+    for (size_t s = 0; s < full.delta.size(); s++) {
+        double a = 0.0;
+        for (int l = 0; l < od; l++) a += excess(full.off[s * od + l]);
+        if (a > R2) continue;
+        S.delta.push_back(full.delta[s]);
+        for (int l = 0; l < od; l++) S.off.push_back(full.off[s * od + l]);
+    }
+    return S;
+}
+
 Consts make_consts(const Geom& g) {
     Consts c;
-    Stencil st[3] = {make_stencil(g, g.r), make_stencil(g, g.r_extra), make_stencil(g, g.r_half)};
+    Stencil st[3] = {screen_update_stencil(g, make_stencil(g, g.r)), make_stencil(g, g.r_extra),
+                     make_stencil(g, g.r_half)};
     for (auto& s : st) c.st_cap = std::max(c.st_cap, (int)s.delta.size());
     const int odp = std::max(g.od, 1);
     const int TW = 2 * g.table_k + 1;
@@ -300,7 +332,7 @@ void prepare(Instance& I, const Geom& g, int max_iter) {
         I.base = nullptr;
         I.cap = 0;
         size_t want = off + off / 8;
-        EGG_CHECK(cudaMalloc(&I.base, want));
+        EGG_CHECK(dev_alloc((void**)&I.base, want));
         I.cap = want;
     }
     layout_work(g, max_iter, (char*)I.base, w, &xin, true);
@@ -367,7 +399,9 @@ __global__ void k_iter_end(Work w, cudaGraphConditionalHandle h, int in_graph, i
 // One iteration of the loop body.  With prof (8 events), the four kernel
 // groups are bracketed by CUDA events on the launching stream.
 // Parts of one iteration: 0 = begin + grid check, 1 = grid sort (skippable
-// when no point changed cell), 2 = the rest.
+// when no point changed cell), 2 = the rest.  In the loop graph part 2 ends
+// at the update (part 3 = the extra check, behind a conditional node; part 4
+// = the loop control).
 void enqueue_part(Instance& I, int part, cudaGraphConditionalHandle h, int in_graph, cudaEvent_t* prof = nullptr) {
     cudaStream_t st = I.st;
     auto mark = [&](int k) {
@@ -383,6 +417,14 @@ void enqueue_part(Instance& I, int part, cudaGraphConditionalHandle h, int in_gr
         launch_build_sort(single(I.g, I.w), st);
         return;
     }
+    if (part == 3) {
+        launch_extra_check(single(I.g, I.w), st, true);
+        return;
+    }
+    if (part == 4) {
+        k_iter_end<<<1, 1, 0, st>>>(I.w, h, in_graph, I.g.stop_rule);
+        return;
+    }
     mark(1);
     mark(2);
     launch_cell_sums(single(I.g, I.w), st);
@@ -392,12 +434,15 @@ void enqueue_part(Instance& I, int part, cudaGraphConditionalHandle h, int in_gr
     mark(4);
     launch_update(single(I.g, I.w), nullptr, st);
     mark(5);
+    if (in_graph) return;  // parts 3 and 4 follow behind the extra check's conditional node
     mark(6);
     launch_extra_check(single(I.g, I.w), st);
     mark(7);
     k_iter_end<<<1, 1, 0, st>>>(I.w, h, in_graph, I.g.stop_rule);
 }
 
+// one iteration outside the loop graph (host-driven loop): parts 0-2, the
+// last of which runs the extra check and the loop control itself
 void enqueue_iteration(Instance& I, cudaGraphConditionalHandle h, int in_graph, cudaEvent_t* prof = nullptr) {
     for (int part = 0; part < 3; part++) enqueue_part(I, part, h, in_graph, prof);
 }
@@ -466,9 +511,42 @@ bool ensure_graph(Instance& I) {
             e = cudaStreamEndCapture(I.st, &captured);
         }
     }
+    // ... -> [rest of the iteration up to the update, gate] -> IF(flag) [extra check] -> [loop control]
+    cudaGraphConditionalHandle hx;
+    cudaGraphNode_t tail2 = nullptr, ifx = nullptr;
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hx, body, 0, 0);
     if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(I.st, body, &ifnode, nullptr, 1, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
         enqueue_part(I, 2, h, 1);
+        launch_gate_extra(I.w, hx, I.st);
+        cudaStreamCaptureStatus cs;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        e = cudaStreamGetCaptureInfo(I.st, &cs, nullptr, nullptr, &deps, &nd);
+        if (e == cudaSuccess && nd == 1) tail2 = deps[0];
+        cudaGraph_t captured = nullptr;
+        const cudaError_t e2 = cudaStreamEndCapture(I.st, &captured);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess && !tail2) e = cudaErrorUnknown;
+    }
+    if (e == cudaSuccess) {
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+        cp.conditional.handle = hx;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        e = cudaGraphAddNode(&ifx, body, &tail2, 1, &cp);
+        if (e == cudaSuccess)
+            e = cudaStreamBeginCaptureToGraph(I.st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            enqueue_part(I, 3, h, 1);
+            cudaGraph_t captured = nullptr;
+            e = cudaStreamEndCapture(I.st, &captured);
+        }
+    }
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(I.st, body, &ifx, nullptr, 1, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        enqueue_part(I, 4, h, 1);
         cudaGraph_t captured = nullptr;
         e = cudaStreamEndCapture(I.st, &captured);
     }
@@ -657,9 +735,10 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
         // grid sort (3 per radix pass + 4), 2 cell sums, need, [2 order
         // parameter], update, 3 extra check, end; then the final build
         // (begin, check, sort), labels (1 or 4 kernels), [2 cell sums + 2
-        // order parameter], [positions].  In the loop graph a gate kernel
-        // runs every iteration and the grid sort only in iterations where
-        // some point changed cell.
+        // order parameter], [positions].  In the loop graph two gate kernels
+        // run every iteration, the grid sort only in iterations where some
+        // point changed cell and the extra check only where the update left
+        // the flag at 1.
         const int sort_l = 3 * plan_count(g) + 4;
         const int build_l = sort_l + 2;
         const int per_iter = sort_l + 1 + 9 + ((g.order_mode == 2 || g.stop_rule == 1) ? 2 : 0);
@@ -669,7 +748,8 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
         if (use_graph) {
             // grid builds in the loop: all builds but the final one when it rebuilt
             const int loop_builds = I.h_ctrl[kCtrlBuilds] - (I.h_ctrl[kCtrlChanged] ? 1 : 0);
-            loop_l = (long long)iters * (per_iter - sort_l + 1) + (long long)loop_builds * sort_l;
+            loop_l = (long long)iters * (per_iter - sort_l - 1) + 3LL * I.h_ctrl[kCtrlExtraRuns] +
+                     (long long)loop_builds * sort_l;
         }
         stats->launches = (int32_t)(2 + loop_l + final_l + (opts.warm_start ? 10 : 0));
         stats->grid_builds = I.h_ctrl[kCtrlBuilds];
@@ -1023,6 +1103,14 @@ __attribute__((visibility("default"))) int egg_release(void) {
 }
 
 __attribute__((visibility("default"))) int egg_abi_version(void) { return EGG_SYNC_ABI_VERSION; }
+
+__attribute__((visibility("default"))) int egg_inject_alloc_failures(int32_t count) {
+    return egg::guarded([&] {
+        if (count < 0) throw egg::ArgError{EGG_ERR_ARG, "count must be >= 0"};
+        egg::g_fail_allocs = count;
+        return (int)EGG_OK;
+    });
+}
 
 __attribute__((visibility("default"))) int egg_update_counters(int64_t* out, int32_t cap) {
 #ifdef EGG_UPDATE_STATS

@@ -31,6 +31,20 @@ struct ArgError {
                                                             std::to_string(__LINE__)}; \
     } while (0)
 
+// Every device allocation of the library goes through dev_alloc.  For tests
+// of the error paths, egg_inject_alloc_failures(k) makes the next k calls
+// fail as cudaMalloc does when the device is out of memory
+// (cudaErrorMemoryAllocation), without allocating anything.
+extern int g_fail_allocs;
+inline cudaError_t dev_alloc(void** p, size_t bytes) {
+    if (g_fail_allocs > 0) {
+        g_fail_allocs--;
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    return cudaMalloc(p, bytes);
+}
+
 // geometry exactly as the reference computes it (EGG_SynC.cu:1249-1260, 1430, 563, 779, 1045)
 Geom make_geom(int64_t n64, int d, float eps);
 

@@ -94,6 +94,9 @@ void launch_need(const Exec& ex, cudaStream_t st);
 void launch_order_param(const Geom& g, const Work& w, int final_slot, cudaStream_t st);
 
 // extra convergence check (egg_extra.cu)
-void launch_extra_check(const Exec& ex, cudaStream_t st);
+void launch_extra_check(const Exec& ex, cudaStream_t st, bool gated = false);
+// loop graph of one instance: opens the conditional node of the extra check
+// when the update left the flag at 1 (stage stamp and run count included)
+void launch_gate_extra(const Work& w, cudaGraphConditionalHandle h, cudaStream_t st);
 
 }  // namespace egg

@@ -499,7 +499,7 @@ struct Scratch {
     template <typename T>
     T* get(size_t cnt) {
         void* p = nullptr;
-        EGG_CHECK(cudaMalloc(&p, std::max<size_t>(cnt, 1) * sizeof(T)));
+        EGG_CHECK(dev_alloc((void**)&p, std::max<size_t>(cnt, 1) * sizeof(T)));
         ptrs.push_back(p);
         return (T*)p;
     }
@@ -553,7 +553,7 @@ FGrid features(const float* X, size_t sp, size_t sl, int n, int d, float eps, vo
         if (B.grid) EGG_CHECK(cudaFree(B.grid));
         B.grid = nullptr;
         B.grid_cap = 0;
-        EGG_CHECK(cudaMalloc(&B.grid, need));
+        EGG_CHECK(dev_alloc((void**)&B.grid, need));
         B.grid_cap = need;
     }
     G.su = (long long*)B.grid;
@@ -579,7 +579,7 @@ void infer(const egg_mlp& m, const __nv_bfloat16* feats, int n, float* out, Buff
         if (B.w) EGG_CHECK(cudaFree(B.w));
         B.w = nullptr;
         B.w_cap = 0;
-        EGG_CHECK(cudaMalloc(&B.w, wbytes));
+        EGG_CHECK(dev_alloc((void**)&B.w, wbytes));
         B.w_cap = wbytes;
     }
     P.base = (float*)B.w;
@@ -619,7 +619,7 @@ void ensure(void** p, size_t* cap, size_t bytes) {
     if (*p) EGG_CHECK(cudaFree(*p));
     *p = nullptr;
     *cap = 0;
-    EGG_CHECK(cudaMalloc(p, bytes));
+    EGG_CHECK(dev_alloc((void**)p, bytes));
     *cap = bytes;
 }
 

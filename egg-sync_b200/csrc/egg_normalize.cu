@@ -89,7 +89,7 @@ int minmax_normalize(const float* x, int64_t n, int32_t d, float* out, float* lo
     std::vector<void*> tmp;
     auto alloc = [&](size_t bytes) {
         void* p = nullptr;
-        EGG_CHECK(cudaMalloc(&p, bytes));
+        EGG_CHECK(dev_alloc((void**)&p, bytes));
         tmp.push_back(p);
         return p;
     };

@@ -204,7 +204,7 @@ int simple_run(const float* x, int64_t n64, int32_t d, float eps, float lam, int
     std::vector<void*> tmp;
     auto alloc = [&](size_t bytes) {
         void* p = nullptr;
-        EGG_CHECK(cudaMalloc(&p, std::max<size_t>(bytes, 4)));
+        EGG_CHECK(dev_alloc((void**)&p, std::max<size_t>(bytes, 4)));
         tmp.push_back(p);
         return p;
     };

@@ -207,6 +207,12 @@ __device__ __forceinline__ void visit_cell(const Geom& g, const Work& w, int c, 
             const float4* xp = w.xp + (size_t)sb * PW;
             const float4* sp = w.smp + (size_t)sb * PS;
             for (int q = sb; q < se; q++, xp += PW, sp += PS) {
+#ifdef EGG_UPDATE_STATS
+                {
+                    const unsigned am_ = __activemask();
+                    if ((threadIdx.x & 31) == __ffs(am_) - 1) a.st[kUsWalkSteps] += 1;
+                }
+#endif
                 float xq[4 * PW];
 #pragma unroll
                 for (int k = 0; k < PW; k++) {
@@ -306,12 +312,18 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
     // for bit: keep the position and the last violation bit.
     const int zb = g.od < d ? gi[g.od] / g.zblk : 0;
     const bool need_me = w.ctrl[kCtrlForce] != 0 || ((w.need[obase] >> zb) & 1ull) != 0;
+    // Xn equals X here unless this iteration rebuilt the grid (the grid check
+    // copied Xn into X; a rebuild reorders X only): a kept position is
+    // written back only after a rebuild (the control word is read where it
+    // is used, so nothing extra stays live over the walk)
     if (!__any_sync(0xffffffffu, need_me)) {
         bool viol = false;
         if (valid) {
-            for (int l = 0; l < d; l++) w.Xn[(size_t)l * g.ns + i] = x[l];
+            if (w.ctrl[kCtrlChanged] != 0)
+                for (int l = 0; l < d; l++) w.Xn[(size_t)l * g.ns + i] = x[l];
             viol = w.viol_orig[w.orig[i]] != 0;
         }
+        if (lane == 0 && w.warp_moved) w.warp_moved[i >> 5] = 0;
         if (__any_sync(0xffffffffu, viol) && lane == 0) {
             volatile int* f = w.ctrl + kCtrlFlag;
             if (*f != 0) *f = 0;
@@ -357,8 +369,20 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
 #ifdef EGG_UPDATE_STATS
     const long long t_walk0 = clock64();
 #endif
+#ifdef EGG_UPDATE_STATS
+    const bool ls_warp = a.st[kUsLaneWarps] == 0;  // meaningful in lane 0, which counts
+    for_candidates(g, w, gi, obase, lane, d, lane_needs, [&](int c) {
+        const long long tv = clock64();
+        visit_cell<D>(g, w, c, x, gi, a, Ts, Tc, Tm, K, TW);
+        if (lane == 0 && ls_warp) {
+            a.st[kUsWarpVisits] += 1;
+            a.st[kUsCyclesVisits] += (unsigned)(clock64() - tv);
+        }
+    });
+#else
     for_candidates(g, w, gi, obase, lane, d, lane_needs,
                    [&](int c) { visit_cell<D>(g, w, c, x, gi, a, Ts, Tc, Tm, K, TW); });
+#endif
 #ifdef EGG_UPDATE_STATS
     {
         const long long dt = clock64() - t_walk0;
@@ -373,7 +397,8 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
     bool moved = false;
     int onew = 0, zbnew = 0;
     if (valid && !walk) {
-        for (int l = 0; l < d; l++) w.Xn[(size_t)l * g.ns + i] = x[l];
+        if (w.ctrl[kCtrlChanged] != 0)
+            for (int l = 0; l < d; l++) w.Xn[(size_t)l * g.ns + i] = x[l];
     } else if (valid) {
         for (int l = 0; l < d; l++) {
             const float corner = __fmul_rn((float)gi[l], g.side);
@@ -410,6 +435,9 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
             atomicOr(dcur + onew, 1ull << zbnew);
         }
     }
+    // the warps whose points moved: the next grid check reads only those
+    const bool warp_mv = __any_sync(0xffffffffu, moved);
+    if (lane == 0 && w.warp_moved) w.warp_moved[i >> 5] = warp_mv ? 1 : 0;
     if (__any_sync(0xffffffffu, viol) && lane == 0) {
         volatile int* f = w.ctrl + kCtrlFlag;
         if (*f != 0) *f = 0;
@@ -423,7 +451,9 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
         // shadow lanes, and lanes that kept their result (their lockstep
         // visits are not work of the update)
         for (int k = 0; k < kUStats; k++)
-            if (k != kUsLaneWarps && k != kUsCyclesShared && k != kUsCyclesLane) a.st[k] = 0;
+            if (k != kUsLaneWarps && k != kUsCyclesShared && k != kUsCyclesLane && k != kUsWarpVisits &&
+                k != kUsCyclesVisits && k != kUsWalkSteps)
+                a.st[k] = 0;
     }
     for (int k = 0; k < kUStats; k++) {
         unsigned long long v = a.st[k];

@@ -26,11 +26,12 @@ EXPORTS = ("egg_opts_default", "egg_sync_run", "egg_sync_step", "egg_sync_grid",
            "egg_sync_batch", "egg_status_str", "egg_last_error", "egg_release", "egg_abi_version",
            "egg_update_counters", "egg_mlp_feature_dim", "egg_mlp_features", "egg_mlp_forward", "egg_mlp_grad",
            "egg_mlp_train", "egg_minmax_normalize", "egg_simple_sync_run", "egg_knn_mean", "egg_mdl_cost",
-           "egg_mdl_search")
+           "egg_mdl_search", "egg_inject_alloc_failures")
 
 # egg_update_counters slots
 UPDATE_COUNTERS = ("points", "cells", "small_pass", "full", "tight_in", "tight_out", "groups_in", "groups_out",
-                   "pairs", "pairs_in", "lane_warps", "half_count", "neighbors", "cycles_shared", "cycles_lane")
+                   "pairs", "pairs_in", "lane_warps", "half_count", "neighbors", "cycles_shared", "cycles_lane",
+                   "warp_visits", "cycles_visits", "walk_steps")
 
 
 class EggMlp(C.Structure):
@@ -130,6 +131,9 @@ def load():
     L.egg_last_error.restype = C.c_char_p
     L.egg_release.argtypes = []
     L.egg_release.restype = C.c_int
+    if hasattr(L, "egg_inject_alloc_failures"):  # testing aid (tests/test_capi.py checks every export)
+        L.egg_inject_alloc_failures.argtypes = [C.c_int32]
+        L.egg_inject_alloc_failures.restype = C.c_int
     L.egg_abi_version.argtypes = []
     L.egg_abi_version.restype = C.c_int
     L.egg_update_counters.argtypes = [C.POINTER(C.c_int64), C.c_int32]

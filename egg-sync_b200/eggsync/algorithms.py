@@ -187,20 +187,25 @@ def egg_step(D, eps: float):
     return out, cnt, (int(flags[0]), int(flags[1]))
 
 
-def egg_grid(D, eps: float):
-    """The double grid of D: (order, cell_of, cell_start) as int32 arrays."""
+def egg_grid(D, eps: float, out=None):
+    """The double grid of D: (order, cell_of, cell_start) as int32 arrays.
+
+    ``out`` (optional): three preallocated int32 buffers (numpy arrays or
+    torch tensors, host or device) of n, n and n + 1 entries; they are
+    filled and returned, cell_start sliced to the n_cells + 1 used entries."""
     L = _lib.load()
     ptr, n, d, keep, dev, stream = _prepare(D)
-    order = np.empty(n, np.int32)
-    cell_of = np.empty(n, np.int32)
-    start = np.empty(n + 1, np.int32)
+    if out is None:
+        out = (np.empty(n, np.int32), np.empty(n, np.int32), np.empty(n + 1, np.int32))
+    order, cell_of, start = out
+    ptrs = [_out_ptr(b, m, np.int32, w) for b, m, w in ((order, n, "order"), (cell_of, n, "cell_of"),
+                                                         (start, n + 1, "cell_start"))]
     M = C.c_int32(0)
     with _DeviceGuard(dev):
-        check(L.egg_sync_grid(C.c_void_p(ptr), n, d, float(eps), C.c_void_p(order.ctypes.data),
-                              C.c_void_p(cell_of.ctypes.data), C.c_void_p(start.ctypes.data), C.byref(M),
-                              C.c_void_p(stream) if stream else None))
+        check(L.egg_sync_grid(C.c_void_p(ptr), n, d, float(eps), C.c_void_p(ptrs[0]), C.c_void_p(ptrs[1]),
+                              C.c_void_p(ptrs[2]), C.byref(M), C.c_void_p(stream) if stream else None))
     del keep
-    return order, cell_of, start[: M.value + 1].copy()
+    return order, cell_of, start[: M.value + 1]
 
 
 def egg_sync_batch(instances, max_iter: int = 0, full_update: bool = False, tune: str = "auto",

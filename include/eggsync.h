@@ -281,6 +281,17 @@ int egg_release(void);
 /* EGG_SYNC_ABI_VERSION of the loaded library. */
 int egg_abi_version(void);
 
+/* Testing aid for the error paths; no counterpart in the reference, whose
+ * failed allocations exit the process (gpuAssert, EGG_SynC.cu:20-26).  The
+ * next `count` device allocations made by any entry point fail as cudaMalloc
+ * does on an exhausted device, without allocating: the call returns
+ * EGG_ERR_CUDA ("out of memory" in egg_last_error()), holds no device memory
+ * from the failed attempt, and the next call allocates again.  Workspaces
+ * are cached, so a call that needs no new workspace allocates nothing (call
+ * egg_release() first to force one).  count 0 clears it; count < 0 is
+ * EGG_ERR_ARG. */
+int egg_inject_alloc_failures(int32_t count);
+
 /* Interaction counters of the update kernel summed over the last
  * egg_sync_run: point updates computed, candidate cells examined, cells
  * passing the reference's small box test, cells aggregated as fully covered,

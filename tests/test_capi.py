@@ -166,3 +166,12 @@ def test_python_front_end_rejects_bad_input(eggsync_lib):
     with pytest.raises(_lib.EggError) as e:
         egg_sync(np.zeros((10, 2), np.float32), 5.0)
     assert e.value.status == _lib.EGG_ERR_GEOMETRY
+
+
+def test_alloc_failure_injection_arguments(eggsync_lib):
+    """The error-path testing aid rejects a negative count and clears with 0
+    (no device needed)."""
+    from eggsync import _lib
+
+    assert eggsync_lib.egg_inject_alloc_failures(-1) == _lib.EGG_ERR_ARG
+    assert eggsync_lib.egg_inject_alloc_failures(0) == _lib.EGG_OK

@@ -15,9 +15,11 @@
   disputed points.  Exact equality is not the bar at these sizes: the
   reference sums cells with float atomics in its own order, and over
   hundreds of iterations pairs of points sit within 1e-7 of eps (the float32
-  rounding of their positions decides whether they are neighbours).  On the
-  500k workload the FP64 oracle's own run disagrees with the reference in
-  one point and with this library in two (lying 4e-8 from a cell face); on
+  rounding of their positions decides whether they are neighbours).  The
+  FP64 oracle's own full runs disagree with the reference too: on the 500k
+  workload in one point (and with this library in two, lying 4e-8 from a
+  cell face), on the 250k workload in 9 points (and with this library in
+  8; this library and the reference differ in 13); on
   the 1M workload 356 of the 387 disputed points are one collapsed group the
   reference merged with its neighbour after such a tie, while this library
   follows the FP64 oracle's step exactly for every one of them in all 191

@@ -1,0 +1,89 @@
+"""The loop on the reference's own real data sets (python/data.py:44-97,
+run_experiment.py:547-551), min-max normalised, at the experiments' eps 0.05.
+
+The data files are not committed: the tests read them from a copy of the
+reference's data/ folder at EGG_REAL_DATA (default: _data/real in the
+repository) and skip when it is absent.
+
+* up to 20,000 points: the same iteration count and the same partition as
+  the FP64 oracle's full run on the CPU;
+* larger sets (eb, 45,781 x 3; Skin_NonSkin, 245,057 x 3): along the loop's
+  own trajectory, at iterations 0, 5, 20 and the last one, 2,000 sampled
+  points agree with the oracle's step from the loop's positions (counts
+  exact, positions within 1e-5), and a repeat run is bit-identical;
+* every set, where the fixture exists: the same partition as the reference
+  EGG-SynC's own run on a B200 (tests/golden/make_golden_real.py), up to
+  the disputed points that float32 ties at eps produce on large sets
+  (bounded at 0.05% of n, as for the large synthetic workloads).
+"""
+import os
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import REPO, load_golden
+from eggsync import data, egg_sync
+from oracle import ari, same_partition
+
+pytestmark = pytest.mark.gpu
+
+DATA = Path(os.environ.get("EGG_REAL_DATA", str(REPO / "_data" / "real")))
+SMALL = [k for k, v in data.REAL.items() if v[2][0] <= 20000]
+LARGE = [k for k, v in data.REAL.items() if v[2][0] > 20000]
+POS_TOL = 1e-5
+
+
+def load(name):
+    f = DATA / data.REAL[name][0]
+    if not f.exists():
+        pytest.skip("real data set %s not present at %s" % (name, DATA))
+    X = data.load_real(name, DATA)
+    assert X.shape == data.REAL[name][2]
+    return X
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_real_small_equals_oracle_run(oracle, name):
+    X = load(name)
+    lab, info = egg_sync(X, data.REAL_EPS)
+    olab, oit, _, _ = oracle.run(X, data.REAL_EPS)
+    assert info["converged"]
+    assert info["iterations"] == oit
+    assert same_partition(lab, olab)
+
+
+@pytest.mark.parametrize("name", LARGE)
+def test_real_large_trajectory_sampled(oracle, name):
+    X = load(name)
+    eps = data.REAL_EPS
+    lab, info = egg_sync(X, eps)
+    T = info["iterations"]
+    idx = np.random.default_rng(3).choice(len(X), 2000, replace=False).astype(np.int32)
+    for k in sorted({k for k in (0, 5, 20) if k < T} | {T - 1}):
+        P = X
+        if k:
+            P = np.empty_like(X)
+            egg_sync(X, eps, max_iter=k, positions_out=P)
+        P1 = np.empty_like(X)
+        egg_sync(X, eps, max_iter=k + 1, positions_out=P1)
+        ox, ocnt, _ = oracle.step_sample(P, eps, idx)
+        assert np.abs(P1[idx] - ox).max() <= POS_TOL, "iteration %d" % k
+    lab2, info2 = egg_sync(X, eps)
+    assert np.array_equal(lab, lab2) and info2["iterations"] == T
+
+
+@pytest.mark.parametrize("name", sorted(data.REAL))
+def test_real_matches_reference_egg(name):
+    from test_gpu_large import disputed_points
+
+    from make_golden import checksum
+
+    G = load_golden("ref_egg_real_%s.npz" % name)
+    X = load(name)
+    assert checksum(X) == G["x_checksum"]
+    lab, info = egg_sync(X, data.REAL_EPS)
+    ref = G["labels"][0]
+    assert info["iterations"] == int(G["iterations"][0])
+    assert ari(lab, ref) >= 0.9999
+    assert len(disputed_points(lab, ref)) <= max(0, int(5e-4 * len(X)))
