@@ -57,10 +57,11 @@ L2_FLUSH_BYTES = 256 << 20
 C5_SYNC_ITERATIONS = 10
 # points in the timed sample of the CPU baseline
 CPU_SAMPLE = 4000
-# DRAM bytes (read + written) of one update launch on this workload, mean over
-# the 191 launches of a run, from one ncu capture of the dram__bytes counters
-# (python bench.py --profile-run under ncu -k regex:k_update).
-UPDATE_DRAM_BYTES_PER_LAUNCH = 22.85e6
+# DRAM bytes (read + written) of one update launch on this workload: the mean
+# of iterations 2-4 (72.1 MB read + 4.8 MB written), from a bounded ncu capture
+# of the dram__bytes counters (ncu -k regex:k_update -s 193 -c 3 on
+# python bench.py --profile-run; cold cache: ncu flushes between replays).
+UPDATE_DRAM_BYTES_PER_LAUNCH = 76.9e6
 
 
 def parse():
@@ -468,8 +469,8 @@ def run_ours(args, rank, local, world, pg):
         "gpu_launches": int(info["launches"]) * args.steps,
         "roofline": {"bound": "hbm", "kernel": "k_update", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": UPDATE_DRAM_BYTES_PER_LAUNCH,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, mean over the 191 "
-                                       "update launches of one run of this workload",
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, mean of the update "
+                                       "launches of iterations 2-4 (-s 193 -c 3), cold cache",
                      "peak_source": peak_kind, "launch_ms": upd_ms,
                      "launches": pinfo["kernel_launches"]["update"],
                      "algorithmic_bytes_per_launch": ub,

@@ -432,17 +432,19 @@ void set_tables(Plan& P, const Config& c) {
     }
 }
 
-// one iteration of every group, then the control kernel
-// one iteration of group k's instances
-void enqueue_group(Plan& P, int k, cudaStream_t st) {
+// one iteration of group k's instances; part 0 = up to the update, 1 = the
+// extra check (in the loop graph behind a conditional node), -1 = both
+void enqueue_group(Plan& P, int k, cudaStream_t st, int part = -1) {
     Group& gr = P.groups[k];
     const Exec ex = batched(gr.act, gr.d);
-    launch_build_check(ex, st, false);  // the control kernel cleared the changed words
-    launch_build_sort(ex, st);
-    launch_cell_sums(ex, st);
-    launch_need(ex, st);
-    launch_update(ex, nullptr, st);
-    launch_extra_check(ex, st);
+    if (part != 1) {
+        launch_build_check(ex, st, false);  // the control kernel cleared the changed words
+        launch_build_sort(ex, st);
+        launch_cell_sums(ex, st);
+        launch_need(ex, st);
+        launch_update(ex, nullptr, st);
+    }
+    if (part != 0) launch_extra_check(ex, st, part == 1);
 }
 
 void enqueue_iteration(State& S, Plan& P, cudaGraphConditionalHandle h, int in_graph) {
@@ -529,12 +531,23 @@ cudaGraphExec_t get_graph(State& S, Plan& P, const Config& c) {
             cp.conditional.size = 1;
             e = cudaGraphAddNode(&ifs[k], body, &gate, 1, &cp);
             if (e != cudaSuccess) break;
-            e = cudaStreamBeginCaptureToGraph(S.st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                              cudaStreamCaptureModeThreadLocal);
+            // group body: [check .. update, gate] -> IF(some instance flagged) [extra check]
+            cudaGraph_t gbody = cp.conditional.phGraph_out[0];
+            cudaGraphConditionalHandle hx;
+            e = cudaGraphConditionalHandleCreate(&hx, gbody, 0, 0);
+            if (e != cudaSuccess) break;
+            e = cudaStreamBeginCaptureToGraph(S.st, gbody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
             if (e != cudaSuccess) break;
             bool ok = true;
+            cudaGraphNode_t tail = nullptr;
             try {
-                enqueue_group(P, k, S.st);
+                enqueue_group(P, k, S.st, 0);
+                launch_batch_gate_extra(batched(P.groups[k].act, P.groups[k].d), hx, S.st);
+                cudaStreamCaptureStatus cs;
+                const cudaGraphNode_t* deps = nullptr;
+                size_t nd = 0;
+                EGG_CHECK(cudaStreamGetCaptureInfo(S.st, &cs, nullptr, nullptr, &deps, &nd));
+                if (nd == 1) tail = deps[0];
             } catch (const CudaError& ce) {
                 ok = false;
                 e = ce.code;
@@ -542,6 +555,26 @@ cudaGraphExec_t get_graph(State& S, Plan& P, const Config& c) {
             cudaGraph_t captured = nullptr;
             const cudaError_t e2 = cudaStreamEndCapture(S.st, &captured);
             if (ok) e = e2;
+            if (e == cudaSuccess && !tail) e = cudaErrorUnknown;
+            if (e != cudaSuccess) break;
+            cudaGraphNodeParams xp = {cudaGraphNodeTypeConditional};
+            xp.conditional.handle = hx;
+            xp.conditional.type = cudaGraphCondTypeIf;
+            xp.conditional.size = 1;
+            cudaGraphNode_t ifx;
+            e = cudaGraphAddNode(&ifx, gbody, &tail, 1, &xp);
+            if (e != cudaSuccess) break;
+            e = cudaStreamBeginCaptureToGraph(S.st, xp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) break;
+            try {
+                enqueue_group(P, k, S.st, 1);
+            } catch (const CudaError& ce) {
+                ok = false;
+                e = ce.code;
+            }
+            const cudaError_t e3 = cudaStreamEndCapture(S.st, &captured);
+            if (ok) e = e3;
         }
         if (e == cudaSuccess) {
             CtlArgs a = ctl_args(P);
@@ -766,16 +799,18 @@ int enqueue_prologue(State& S, Plan& P, int max_iter) {
 // tables), cell sums (2), need, update, extra check (3)
 int group_launches(const Group& gr) { return 1 + 3 * gr.act.max_passes + 4 + 2 + 1 + 1 + 3; }
 
-// Kernels of the loop: gate and control every iteration, and each group's
-// kernels in the iterations where it had active instances (the largest
-// iteration count among its instances; an idle group's conditional node
-// launches nothing).
+// Kernels of the loop graph: gate and control every iteration, and each
+// group's kernels in the iterations where it had active instances (the
+// largest iteration count among its instances; an idle group's conditional
+// node launches nothing): the extra-check gate every such iteration, the
+// three extra-check kernels only where an instance's flag reached it
+// (counted once per instance: its final iteration).
 long long loop_launches(const Plan& P, int loop_iters, const std::vector<int>& res) {
     long long l = 2LL * loop_iters;
     for (const Group& gr : P.groups) {
         int m = 0;
         for (int pos = gr.begin; pos < gr.end; pos++) m = std::max(m, res[5 * (size_t)pos]);
-        l += (long long)m * group_launches(gr);
+        l += (long long)m * (group_launches(gr) - 3 + 1) + 3LL * (gr.end - gr.begin);
     }
     return l;
 }

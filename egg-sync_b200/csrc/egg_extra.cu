@@ -240,8 +240,8 @@ __global__ void __launch_bounds__(128) k_ball_bbox(Geom g, Work w, int mark) {
     ball_bbox_body<D>(g, w, blockIdx.x, gridDim.x, mark);
 }
 template <int D>
-__global__ void __launch_bounds__(128) kb_ball_bbox(BatchArgs B) {
-    batch_for(B, [&](const Geom& g, const Work& w, int bx, int gx) { ball_bbox_body<D>(g, w, bx, gx); });
+__global__ void __launch_bounds__(128) kb_ball_bbox(BatchArgs B, int mark) {
+    batch_for(B, [&](const Geom& g, const Work& w, int bx, int gx) { ball_bbox_body<D>(g, w, bx, gx, mark); });
 }
 __global__ void __launch_bounds__(256) k_cell_ballbox(Geom g, Work w) { cell_ballbox_body(g, w, blockIdx.x, gridDim.x); }
 __global__ void __launch_bounds__(256) kb_cell_ballbox(BatchArgs B) {
@@ -282,6 +282,32 @@ void launch_gate_extra(const Work& w, cudaGraphConditionalHandle h, cudaStream_t
     k_gate_extra<<<1, 1, 0, st>>>(w, h);
 }
 
+// The same for one dimension group of a batched loop: one thread per active
+// instance stamps the stage and counts a flagged instance's extra check; the
+// node opens when any of them has its flag at 1.
+__global__ void __launch_bounds__(1024) k_batch_gate_extra(const Work* __restrict__ works,
+                                                           const int* __restrict__ active, const int* __restrict__ nact,
+                                                           cudaGraphConditionalHandle h) {
+    const int na = *nact;
+    const unsigned long long now = globaltimer();
+    int flagged = 0;
+    for (int t = threadIdx.x; t < na; t += blockDim.x) {
+        const Work& w = works[active[t]];
+        const int it = w.ctrl[kCtrlIter];
+        w.stamps[4 * it + 2] = now;
+        if (w.ctrl[kCtrlFlag] != 0) {
+            atomicAdd(w.ctrl + kCtrlExtraRuns, 1);
+            flagged = 1;
+        }
+    }
+    const int any = __syncthreads_or(flagged);
+    if (threadIdx.x == 0) cudaGraphSetConditional(h, any ? 1u : 0u);
+}
+
+void launch_batch_gate_extra(const Exec& ex, cudaGraphConditionalHandle h, cudaStream_t st) {
+    k_batch_gate_extra<<<1, 1024, 0, st>>>(ex.bt->works, ex.bt->active, ex.bt->nact, h);
+}
+
 // The kernels return at once unless the update left the flag at 1; the
 // grids are bounded so that the common early exit costs little.  gated: the
 // call sits behind k_gate_extra, which did the stage stamp and the count.
@@ -289,7 +315,7 @@ void launch_extra_check(const Exec& ex, cudaStream_t st, bool gated) {
     const int blocks = ex.blocks(kShapeCapN128, 128);
     if (ex.batch()) {
         const BatchArgs B = ex.args(kShapeCapN128);
-        EGG_DISPATCH_D(ex.d, kb_ball_bbox, <<<blocks, 128, 0, st>>>(B));
+        EGG_DISPATCH_D(ex.d, kb_ball_bbox, <<<blocks, 128, 0, st>>>(B, gated ? 0 : 1));
         kb_cell_ballbox<<<ex.blocks(kShapeCapN128, 256), 256, 0, st>>>(B);
         EGG_DISPATCH_D(ex.d, kb_annulus, <<<blocks, 128, 0, st>>>(B));
     } else {

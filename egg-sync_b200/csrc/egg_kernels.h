@@ -98,5 +98,7 @@ void launch_extra_check(const Exec& ex, cudaStream_t st, bool gated = false);
 // loop graph of one instance: opens the conditional node of the extra check
 // when the update left the flag at 1 (stage stamp and run count included)
 void launch_gate_extra(const Work& w, cudaGraphConditionalHandle h, cudaStream_t st);
+// loop graph of a batch: the same per dimension group (any active instance flagged)
+void launch_batch_gate_extra(const Exec& ex, cudaGraphConditionalHandle h, cudaStream_t st);
 
 }  // namespace egg

@@ -22,10 +22,6 @@
 // every cost is reproducible bit for bit from run to run.
 #include <cuda_runtime.h>
 
-#include <cub/device/device_radix_sort.cuh>
-#include <cub/device/device_scan.cuh>
-#include <cub/device/device_segmented_reduce.cuh>
-#include <cub/device/device_select.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -36,6 +32,7 @@
 #include "eggsync.h"
 #include "egg_common.cuh"
 #include "egg_host_common.h"
+#include "egg_sort.h"
 
 namespace egg {
 
@@ -175,11 +172,9 @@ __global__ void k_label_keys(const int* __restrict__ labels, int n, unsigned* __
     }
 }
 
-__global__ void k_heads(const unsigned* __restrict__ keys, int m, int* __restrict__ head, int* __restrict__ iota) {
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+__global__ void k_heads(const unsigned* __restrict__ keys, int m, int* __restrict__ head) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x)
         head[j] = (j == 0 || keys[j] != keys[j - 1]) ? 1 : 0;
-        iota[j] = j;
-    }
 }
 
 // first sorted position holding an outlier key (the clustered count)
@@ -204,6 +199,20 @@ __global__ void k_gather_sorted(const float* __restrict__ x, int d, const int* _
 }
 
 // segment of every clustered point: seg[j] = (inclusive count of heads) - 1
+// float32 bits -> unsigned keys in the same order (negative values flipped)
+__global__ void k_float_keys(const float* __restrict__ v, int n, unsigned* __restrict__ keys) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned u = __float_as_uint(v[i]);
+        keys[i] = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    }
+}
+
+// first sorted position of every segment: begin[incl[j] - 1] = j at heads
+__global__ void k_seg_begin(const int* __restrict__ head, const int* __restrict__ incl, int m, int* __restrict__ begin) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x)
+        if (head[j]) begin[incl[j] - 1] = j;
+}
+
 __global__ void k_seg_of(const int* __restrict__ incl, int m, int* __restrict__ seg) {
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) seg[j] = incl[j] - 1;
 }
@@ -274,7 +283,7 @@ struct Arena {
     template <typename T>
     T* get(size_t count) {
         void* p = nullptr;
-        EGG_CHECK(cudaMalloc(&p, std::max<size_t>(1, count * sizeof(T))));
+        EGG_CHECK(dev_alloc((void**)&p, std::max<size_t>(1, count * sizeof(T))));
         ptrs.push_back(p);
         return (T*)p;
     }
@@ -282,15 +291,6 @@ struct Arena {
         for (void* p : ptrs) cudaFree(p);
     }
 };
-
-// CUB's two-phase calls: size query, then the call with scratch from the arena
-template <typename F>
-void cub_call(Arena& A, F&& f) {
-    size_t bytes = 0;
-    EGG_CHECK(f(nullptr, bytes));
-    void* tmp = A.get<char>(bytes);
-    EGG_CHECK(f(tmp, bytes));
-}
 
 // the input on the device (a copy when it is in host memory)
 const float* device_input(Arena& A, const float* x, size_t count, cudaStream_t st) {
@@ -346,7 +346,9 @@ void knn_mean(Arena& A, const float* xd, int n, int d, int k, double out[2], cud
 // percentile with linear interpolation (scipy.stats.iqr).
 std::vector<double> bandwidths(Arena& A, const float* xd, int n, int d, cudaStream_t st) {
     float* col = A.get<float>(n);
-    float* sorted = A.get<float>(n);
+    unsigned* ckeys = A.get<unsigned>(n);
+    unsigned* sorted = A.get<unsigned>(n);  // the column's order-preserving keys, sorted
+    void* sort_tmp = A.get<char>(prim::sort_scratch_bytes(n));
     double* part = A.get<double>(kSumBlocks);
     double* res = A.get<double>(2);
     int* bad = A.get<int>(1);
@@ -360,19 +362,25 @@ std::vector<double> bandwidths(Arena& A, const float* xd, int n, int d, cudaStre
         k_sum_final<<<1, 256, 0, st>>>(part, nb, 1.0 / n, res);
         k_sum_partial<<<nb, 256, 0, st>>>(col, n, 1, res, 2, part);
         k_sum_final<<<1, 256, 0, st>>>(part, nb, 1.0 / (n - 1), res + 1);
-        cub_call(A, [&](void* t, size_t& b) {
-            return cub::DeviceRadixSort::SortKeys(t, b, col, sorted, n, 0, 32, st);
-        });
+        k_float_keys<<<grid_for((size_t)n, 256), 256, 0, st>>>(col, n, ckeys);
+        prim::sort_pairs(ckeys, nullptr, sorted, nullptr, n, sort_tmp, st);
         double mv[2];
         EGG_CHECK(cudaMemcpyAsync(mv, res, 16, cudaMemcpyDeviceToHost, st));
         auto pct = [&](double q) {
             const double pos = q * (double)(n - 1);
             const int lo = (int)std::floor(pos);
             const int hi = std::min(lo + 1, n - 1);
-            float a = 0.f, b = 0.f;
-            EGG_CHECK(cudaMemcpyAsync(&a, sorted + lo, 4, cudaMemcpyDeviceToHost, st));
-            EGG_CHECK(cudaMemcpyAsync(&b, sorted + hi, 4, cudaMemcpyDeviceToHost, st));
+            unsigned ka = 0, kb = 0;
+            EGG_CHECK(cudaMemcpyAsync(&ka, sorted + lo, 4, cudaMemcpyDeviceToHost, st));
+            EGG_CHECK(cudaMemcpyAsync(&kb, sorted + hi, 4, cudaMemcpyDeviceToHost, st));
             EGG_CHECK(cudaStreamSynchronize(st));
+            auto unkey = [](unsigned k) {
+                const unsigned u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+                float f;
+                memcpy(&f, &u, 4);
+                return f;
+            };
+            const float a = unkey(ka), b = unkey(kb);
             const double t = pos - lo;
             // numpy's linear interpolation, from the nearer end
             return t >= 0.5 ? (double)b - ((double)b - a) * (1.0 - t) : (double)a + ((double)b - a) * t;
@@ -401,18 +409,19 @@ struct CostWs {
     Arena A;
     int n, d;
     unsigned *keys, *keys_s;
-    int *idx, *idx_s, *head, *iota, *incl, *seg, *begin, *scal;  // scal: bad flag, m, K
+    int *idx, *idx_s, *head, *incl, *seg, *begin, *scal;  // scal: bad flag, m
     float *xs, *invh;
     double *f, *lf, *sf, *slf;
-    void* tmp = nullptr;
-    size_t tmp_bytes = 0;
+    void* sort_tmp = nullptr;  // scratch of the label sort
+    void* scan_tmp = nullptr;  // scratch of the head scan
     CostWs(int n_, int d_) : n(n_), d(d_) {
+        sort_tmp = A.get<char>(prim::sort_scratch_bytes(n));
+        scan_tmp = A.get<char>(prim::scan_scratch_bytes(n));
         keys = A.get<unsigned>(n);
         keys_s = A.get<unsigned>(n);
         idx = A.get<int>(n);
         idx_s = A.get<int>(n);
         head = A.get<int>(n);
-        iota = A.get<int>(n);
         incl = A.get<int>(n);
         seg = A.get<int>(n);
         begin = A.get<int>((size_t)n + 1);
@@ -423,17 +432,6 @@ struct CostWs {
         lf = A.get<double>(n);
         sf = A.get<double>(n);
         slf = A.get<double>(n);
-    }
-    // CUB's two-phase calls with one growing scratch buffer
-    template <typename F>
-    void cub(F&& fn) {
-        size_t bytes = 0;
-        EGG_CHECK(fn(nullptr, bytes));
-        if (bytes > tmp_bytes) {
-            tmp = A.get<char>(bytes);
-            tmp_bytes = bytes;
-        }
-        EGG_CHECK(fn(tmp, bytes));
     }
 };
 
@@ -447,12 +445,9 @@ double mdl_cost(CostWs& W, const float* xd, const int* labels_d, const std::vect
     const int n = W.n, d = W.d;
     int* bad = W.scal;
     int* dm = W.scal + 1;
-    int* nseg = W.scal + 2;
     EGG_CHECK(cudaMemsetAsync(bad, 0, 4, st));
     k_label_keys<<<grid_for((size_t)n, 256), 256, 0, st>>>(labels_d, n, W.keys, W.idx, bad);
-    W.cub([&](void* t, size_t& b) {
-        return cub::DeviceRadixSort::SortPairs(t, b, W.keys, W.keys_s, W.idx, W.idx_s, n, 0, 32, st);
-    });
+    prim::sort_pairs(W.keys, W.idx, W.keys_s, W.idx_s, n, W.sort_tmp, st);
     // clustered points: keys below 0xffffffff
     k_first_outlier<<<1, 1, 0, st>>>(W.keys_s, n, dm);
     int hs2[2];
@@ -467,15 +462,13 @@ double mdl_cost(CostWs& W, const float* xd, const int* labels_d, const std::vect
     double LD = (double)outliers * std::pow(2.0 * M_PI, -0.5) * prodh;
     *clusters = 0;
     if (m > 0) {
-        k_heads<<<grid_for((size_t)m, 256), 256, 0, st>>>(W.keys_s, m, W.head, W.iota);
-        W.cub([&](void* t, size_t& b) {
-            return cub::DeviceSelect::Flagged(t, b, W.iota, W.head, W.begin, nseg, m, st);
-        });
-        W.cub([&](void* t, size_t& b) { return cub::DeviceScan::InclusiveSum(t, b, W.head, W.incl, m, st); });
+        k_heads<<<grid_for((size_t)m, 256), 256, 0, st>>>(W.keys_s, m, W.head);
+        prim::inclusive_scan(W.head, W.incl, m, W.scan_tmp, st);
+        k_seg_begin<<<grid_for((size_t)m, 256), 256, 0, st>>>(W.head, W.incl, m, W.begin);
         k_seg_of<<<grid_for((size_t)m, 256), 256, 0, st>>>(W.incl, m, W.seg);
         k_gather_sorted<<<grid_for((size_t)m * d, 256), 256, 0, st>>>(xd, d, W.idx_s, m, W.xs);
         int K = 0;
-        EGG_CHECK(cudaMemcpyAsync(&K, nseg, 4, cudaMemcpyDeviceToHost, st));
+        EGG_CHECK(cudaMemcpyAsync(&K, W.incl + (m - 1), 4, cudaMemcpyDeviceToHost, st));
         EGG_CHECK(cudaStreamSynchronize(st));
         // begin[K] = m and the inverse bandwidths, one small upload
         std::vector<int> up(1 + d);
@@ -490,12 +483,8 @@ double mdl_cost(CostWs& W, const float* xd, const int* labels_d, const std::vect
         EGG_MDL_DISPATCH_D(d, k_kde, <<<(m + 255) / 256, 256, 0, st>>>(W.xs, m, d, W.seg, W.begin, W.invh, norm,
                                                                          W.f, W.lf));
         EGG_CHECK(cudaGetLastError());
-        W.cub([&](void* t, size_t& b) {
-            return cub::DeviceSegmentedReduce::Sum(t, b, W.f, W.sf, K, W.begin, W.begin + 1, st);
-        });
-        W.cub([&](void* t, size_t& b) {
-            return cub::DeviceSegmentedReduce::Sum(t, b, W.lf, W.slf, K, W.begin, W.begin + 1, st);
-        });
+        prim::segment_sums(W.f, W.begin, K, W.sf, st);
+        prim::segment_sums(W.lf, W.begin, K, W.slf, st);
         std::vector<int> hb(K + 1);
         std::vector<double> hs(K), hl(K);
         EGG_CHECK(cudaMemcpyAsync(hb.data(), W.begin, 4 * (size_t)(K + 1), cudaMemcpyDeviceToHost, st));

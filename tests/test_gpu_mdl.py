@@ -117,3 +117,46 @@ def test_search_device_input_same_result():
     lab_d, info_d = mdl_search(torch.from_numpy(X).cuda(), 4, max_candidates=6, labels_out=out)
     assert np.array_equal(lab, out.cpu().numpy())
     assert info_d["costs"] == info["costs"] and info_d["eps"] == info["eps"]
+
+
+def test_search_against_reference_sync():
+    """Against the reference's own Sync(D, 5) (python/SynCTorch.py:349-372;
+    fixture ref_sync_search.npz, tests/golden/make_sync_golden.py) on the
+    four ref_mdl inputs: the eps schedule agrees (float32 steps from NN(5)
+    and NN(6)), and both searches end at their first single-cluster
+    clustering.  The candidates are clustered differently (the reference with
+    its Python SynC: neighbours at distance < eps, stop when the mean order
+    parameter exceeds lambda, clusters = groups of allclose points; here with
+    EGG-SynC), so a few candidates' cluster counts differ (s1: 3 vs 2 at the
+    second eps; s2: several of 4 vs 3); the number of candidates and the
+    chosen candidate are the same.  EGG_PARITY_REPORT receives both
+    searches' records."""
+    import json
+    import os
+
+    from conftest import load_golden
+
+    G = load_golden("ref_sync_search.npz")
+    R = load_golden("ref_mdl.npz")
+    rows = []
+    for name in ("s0", "s1", "s2", "s3"):
+        X = R[name + "_X"]
+        ref_eps = G[name + "_eps"]
+        lab, info = mdl_search(X, int(G["k"]))
+        ours = np.array(info["eps"][: info["candidates"]], np.float64)
+        m = min(len(ours), len(ref_eps))
+        assert np.allclose(ours[:m], ref_eps[:m], rtol=1e-5, atol=0)
+        assert info["end_reason"] == "one cluster" and info["clusters"][info["candidates"] - 1] == 1
+        assert int(G[name + "_nclusters"][-1]) == 1
+        # on these inputs both searches end after the same number of
+        # candidates and pick the same one (the last, one cluster)
+        assert info["candidates"] == len(ref_eps)
+        assert info["best"] == int(G[name + "_best"])
+        rows.append({"input": name, "n": len(X), "ref_candidates": len(ref_eps), "ref_best": int(G[name + "_best"]),
+                     "ref_clusters": G[name + "_nclusters"].tolist(), "candidates": info["candidates"],
+                     "best": info["best"], "clusters": info["clusters"][: info["candidates"]]})
+    rep = os.environ.get("EGG_PARITY_REPORT")
+    if rep:
+        with open(rep, "a") as f:
+            for r in rows:
+                f.write(json.dumps(r) + "\n")

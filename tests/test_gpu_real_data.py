@@ -11,10 +11,16 @@ repository) and skip when it is absent.
   own trajectory, at iterations 0, 5, 20 and the last one, 2,000 sampled
   points agree with the oracle's step from the loop's positions (counts
   exact, positions within 1e-5), and a repeat run is bit-identical;
-* every set, where the fixture exists: the same partition as the reference
-  EGG-SynC's own run on a B200 (tests/golden/make_golden_real.py), up to
-  the disputed points that float32 ties at eps produce on large sets
-  (bounded at 0.05% of n, as for the large synthetic workloads).
+* every set: the same partition and iteration count as the reference
+  EGG-SynC's own run on a B200 (tests/golden/make_golden_real.py; two runs
+  each, one partition), with two recorded exceptions, both rounding ties:
+  on iris, points 33 and 114 are mirror images around 0.5 in the third
+  feature and synchronise onto x = 0.5 exactly, a cell face (0.5 / side =
+  40): the FP64 oracle and this library put both in one cell (a 2-point
+  cluster), the reference's float32 sums leave them on either side of the
+  face (two singletons); on Skin_NonSkin the partitions are identical but
+  the reference's flag and extra check first pass at iteration 343, here at
+  345.
 """
 import os
 from pathlib import Path
@@ -32,6 +38,9 @@ DATA = Path(os.environ.get("EGG_REAL_DATA", str(REPO / "_data" / "real")))
 SMALL = [k for k, v in data.REAL.items() if v[2][0] <= 20000]
 LARGE = [k for k, v in data.REAL.items() if v[2][0] > 20000]
 POS_TOL = 1e-5
+# rounding ties where this library (with the FP64 oracle) and the reference
+# part ways; see the module docstring
+KNOWN = {"iris": {"disputed": [33, 114]}, "skin_nonskin": {"iterations": (345, 343)}}
 
 
 def load(name):
@@ -84,6 +93,6 @@ def test_real_matches_reference_egg(name):
     assert checksum(X) == G["x_checksum"]
     lab, info = egg_sync(X, data.REAL_EPS)
     ref = G["labels"][0]
-    assert info["iterations"] == int(G["iterations"][0])
-    assert ari(lab, ref) >= 0.9999
-    assert len(disputed_points(lab, ref)) <= max(0, int(5e-4 * len(X)))
+    known = KNOWN.get(name, {})
+    assert disputed_points(lab, ref).tolist() == known.get("disputed", [])
+    assert (info["iterations"], int(G["iterations"][0])) == known.get("iterations", (info["iterations"],) * 2)
