@@ -82,6 +82,8 @@ struct Work {
     int* orig_tmp;     // [ns]
     int* perm;         // [ns]   radix sort output: new position -> previous position
     int* perm_tmp;     // [ns]
+    unsigned* skey[2]; // [ns] each: whole 32-bit sort keys of the one-key grid sort (d <= 3 and at most
+                       // 256 cells per dimension; nullptr otherwise: the per-dimension passes)
     int* cell_of;      // [ns]   cell index of sorted point i
     // cells (index < M, M only known on the device)
     int* cell_start;   // [ns+1]

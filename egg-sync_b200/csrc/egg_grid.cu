@@ -269,6 +269,112 @@ __device__ __forceinline__ void radix_scatter_body(const Geom& g, const Work& w,
     }
 }
 
+// ---------------------------------------------------------------------------
+// One-key grid sort (d <= 3, at most 256 cells per dimension): the whole sort
+// key of a point -- the sub-cell digit in bits 0-7, then the cell
+// coordinates in the order of the per-dimension passes (plan_pass), 8 bits
+// each -- fits in 32 bits, so it is computed once and the LSD passes move
+// (key, previous position) pairs with coalesced reads instead of recomputing
+// every pass's digit through the permutation.  The digits and their order
+// are those of the per-dimension passes and every pass is stable, so the
+// resulting permutation is the same.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int onekey_passes(const Geom& g) { return 1 + g.d; }
+
+// keys of the points in their current order; the first pass's payload (the
+// identity) goes to the buffer that makes the last pass end in perm
+__device__ __forceinline__ void onekey_keys_body(const Geom& g, const Work& w, int bx, int gx) {
+    EGG_SKIP_IF_UNCHANGED(w.ctrl);
+    const int P = onekey_passes(g);
+    int* v0 = (P & 1) ? w.perm_tmp : w.perm;
+    for (int i = bx * blockDim.x + threadIdx.x; i < g.n; i += gx * blockDim.x) {
+        unsigned key = (unsigned)digit_of(g, w.Xn, i, -1, 0);
+        for (int p = 1; p < P; p++) {
+            int dim, shift;
+            plan_pass(g, p, dim, shift);
+            key |= (unsigned)(cell_dim(__ldg(w.Xn + (size_t)dim * g.ns + i), g) & 255) << (8 * p);
+        }
+        w.skey[0][i] = key;
+        v0[i] = i;
+    }
+}
+
+__device__ __forceinline__ void onekey_hist_body(const Geom& g, const Work& w, int p, int bx) {
+    EGG_SKIP_IF_UNCHANGED(w.ctrl);
+    __shared__ int h[256];
+    const int tiles = (g.n + kSortTile - 1) / kSortTile;
+    const unsigned* kin = w.skey[p & 1];
+    for (int t = threadIdx.x; t < 256; t += blockDim.x) h[t] = 0;
+    __syncthreads();
+    const int b = bx * kSortTile, e = min(b + kSortTile, g.n);
+    for (int i = b + threadIdx.x; i < e; i += blockDim.x) atomicAdd(&h[(__ldg(kin + i) >> (8 * p)) & 255u], 1);
+    __syncthreads();
+    for (int t = threadIdx.x; t < 256; t += blockDim.x) w.hist[(size_t)t * tiles + bx] = h[t];
+}
+
+// stable scatter of one tile of (key, previous position) pairs
+__device__ __forceinline__ void onekey_scatter_body(const Geom& g, const Work& w, int p, int bx) {
+    EGG_SKIP_IF_UNCHANGED(w.ctrl);
+    constexpr int kWarps = kSortThreads / 32;
+    __shared__ int base[256];
+    __shared__ int run[256];
+    __shared__ int wcnt[kWarps][256];
+    const int P = onekey_passes(g);
+    const int tiles = (g.n + kSortTile - 1) / kSortTile;
+    const unsigned* kin = w.skey[p & 1];
+    unsigned* kout = w.skey[(p + 1) & 1];
+    // payload ping-pong that ends in perm: pass p writes perm when P - 1 - p is even
+    const int* vin = ((P - p) & 1) ? w.perm_tmp : w.perm;
+    int* vout = ((P - 1 - p) & 1) ? w.perm_tmp : w.perm;
+    const int shift = 8 * p;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    {
+        const int v = w.digit_total[tid];
+        const int db = block_exclusive_scan(v, nullptr);
+        base[tid] = db + w.hist[(size_t)tid * tiles + bx];
+        run[tid] = 0;
+#pragma unroll
+        for (int k = 0; k < kWarps; k++) wcnt[k][tid] = 0;
+    }
+    __syncthreads();
+    const int tile0 = bx * kSortTile;
+    for (int round = 0; round < kSortTile / kSortThreads; round++) {
+        if (tile0 + round * kSortThreads >= g.n) break;  // uniform across the block
+        const int i = tile0 + round * kSortThreads + tid;
+        const bool valid = i < g.n;
+        unsigned key = 0;
+        int dg = 0;
+        if (valid) {
+            key = __ldg(kin + i);
+            dg = (int)((key >> shift) & 255u);
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, valid ? dg : 256 + lane);
+        const int rank = __popc(peers & lanemask_lt());
+        if (valid && rank == 0) wcnt[wid][dg] = __popc(peers);
+        __syncthreads();
+        {
+            int r = run[tid];
+#pragma unroll
+            for (int k = 0; k < kWarps; k++) {
+                const int c = wcnt[k][tid];
+                wcnt[k][tid] = r;
+                r += c;
+            }
+            run[tid] = r;
+        }
+        __syncthreads();
+        if (valid) {
+            const int pos = base[dg] + wcnt[wid][dg] + rank;
+            if (p + 1 < P) kout[pos] = key;
+            vout[pos] = __ldg(vin + i);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kWarps; k++) wcnt[k][tid] = 0;
+        __syncthreads();
+    }
+}
+
 // gather into the new order and count cell heads per block
 template <int D>
 __device__ __forceinline__ void gather_heads_body(const Geom& g, const Work& w, int identity, int bx) {
@@ -764,6 +870,13 @@ __global__ void __launch_bounds__(kSortThreads) kb_radix_scatter(BatchArgs B, in
                            bx);
     });
 }
+__global__ void __launch_bounds__(256) k_onekey_keys(Geom g, Work w) { onekey_keys_body(g, w, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(kSortThreads) k_onekey_hist(Geom g, Work w, int p) {
+    onekey_hist_body(g, w, p, blockIdx.x);
+}
+__global__ void __launch_bounds__(kSortThreads) k_onekey_scatter(Geom g, Work w, int p) {
+    onekey_scatter_body(g, w, p, blockIdx.x);
+}
 template <int D>
 __global__ void __launch_bounds__(kHeadsBlock) k_gather_heads(Geom g, Work w) {
     gather_heads_body<D>(g, w, 0, blockIdx.x);
@@ -865,6 +978,17 @@ void launch_build_sort(const Exec& ex, cudaStream_t st) {
             kb_radix_hist<<<ex.blocks(kShapeTiles, kSortThreads), kSortThreads, 0, st>>>(ex.args(kShapeTiles), p);
             kb_radix_scan<<<ex.blocks(kShapeDigits, 256), 256, 0, st>>>(ex.args(kShapeDigits), p);
             kb_radix_scatter<<<ex.blocks(kShapeTiles, kSortThreads), kSortThreads, 0, st>>>(ex.args(kShapeTiles), p);
+        }
+    } else if (ex.w->skey[0] != nullptr && ex.g->d <= 3 && ex.g->width <= 256) {
+        // one 32-bit key per point, 1 + d coalesced (key, position) passes
+        const Geom& g = *ex.g;
+        const int tiles = shape_blocks(kShapeTiles, g);
+        const int kb = std::min((g.n + 255) / 256, 148 * 16);
+        k_onekey_keys<<<kb, 256, 0, st>>>(g, *ex.w);
+        for (int p = 0; p < 1 + g.d; p++) {
+            k_onekey_hist<<<tiles, kSortThreads, 0, st>>>(g, *ex.w, p);
+            k_radix_scan<<<shape_blocks(kShapeDigits, g), 256, 0, st>>>(g, *ex.w);
+            k_onekey_scatter<<<tiles, kSortThreads, 0, st>>>(g, *ex.w, p);
         }
     } else {
         const Geom& g = *ex.g;

@@ -169,6 +169,10 @@ size_t layout_work(const Geom& g, int max_iter, char* base, Work& w, float** xin
     add((void**)&w.orig_tmp, 4 * ns);
     add((void**)&w.perm, 4 * ns);
     add((void**)&w.perm_tmp, 4 * ns);
+    const bool one_key = d <= 3 && g.width <= 256;
+    add((void**)&w.skey[0], one_key ? 4 * ns : 0);
+    add((void**)&w.skey[1], one_key ? 4 * ns : 0);
+    if (!one_key) w.skey[0] = w.skey[1] = nullptr;  // the per-dimension passes
     add((void**)&w.cell_of, 4 * ns);
     add((void**)&w.cell_start, 4 * (ns + 1));
     add((void**)&w.cell_dims, 4 * d * ns);
