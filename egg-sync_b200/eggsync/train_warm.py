@@ -1,6 +1,6 @@
 """Train the warm-start network on trajectories of the plain loop.
 
-    python -m eggsync.train_warm [--instances 40] [--sample 25000] [--k 8]
+    python -m eggsync.train_warm [--instances 200] [--sample 25000] [--k 8]
                                  [--epochs 30] [--out PATH]
 
 Training instances are data.train_instance(seed) for seeds 1,000,000 + i
@@ -23,7 +23,7 @@ from . import warm
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--instances", type=int, default=40)
+    ap.add_argument("--instances", type=int, default=200)
     ap.add_argument("--val-instances", type=int, default=4)
     ap.add_argument("--sample", type=int, default=25000)
     ap.add_argument("--k", type=int, default=8)
