@@ -833,7 +833,22 @@ EGG_WRAP0(scan_block_sums, 1024, scan_block_sums_body(g, w))
 __global__ void __launch_bounds__(256) k_radix_scan(Geom g, Work w) { radix_scan_body(g, w, blockIdx.x); }
 EGG_WRAPD(heads_finalize, kHeadsBlock, heads_finalize_body<D>(g, w, bx))
 EGG_WRAP0(outer_ranges, 256, outer_ranges_body(g, w, bx, gx))
-EGG_WRAPD(cell_sums, 256, cell_sums_body<D>(g, w, bx))
+// single instance: a grid capped at 148 x 8 blocks strides over the
+// 256-point blocks (late in a run nearly every warp returns at once, and a
+// full-size grid would be mostly block scheduling); batched: one virtual
+// block each
+template <int D>
+__global__ void __launch_bounds__(256) k_cell_sums(Geom g, Work w) {
+    const int nblk = (g.n + 255) / 256;
+    for (int bx = blockIdx.x; bx < nblk; bx += gridDim.x) cell_sums_body<D>(g, w, bx);
+}
+template <int D>
+__global__ void __launch_bounds__(256) kb_cell_sums(BatchArgs B) {
+    batch_for(B, [&](const Geom& g, const Work& w, int bx, int gx) {
+        (void)gx;
+        cell_sums_body<D>(g, w, bx);
+    });
+}
 EGG_WRAPD(cell_sums_fix, 256, cell_sums_fix_body<D>(g, w, bx, gx))
 
 __global__ void __launch_bounds__(kSortThreads) k_radix_hist(Geom g, Work w, int in_sel, int first, int dim,
@@ -1010,7 +1025,12 @@ void launch_build_sort(const Exec& ex, cudaStream_t st) {
 }
 
 void launch_cell_sums(const Exec& ex, cudaStream_t st) {
-    EGG_GO_D(ex, kShapeN256, 256, st, cell_sums);
+    if (ex.batch()) {
+        EGG_DISPATCH_D(ex.d, kb_cell_sums, <<<ex.blocks(kShapeN256, 256), 256, 0, st>>>(ex.args(kShapeN256)));
+    } else {
+        const int blocks = std::min(shape_blocks(kShapeN256, *ex.g), 148 * 8);
+        EGG_DISPATCH_D(ex.d, k_cell_sums, <<<blocks, 256, 0, st>>>(*ex.g, *ex.w));
+    }
     EGG_GO_D(ex, kShapeFix, 256, st, cell_sums_fix);
 }
 

@@ -279,6 +279,8 @@ namespace {
 struct Instance {
     int dev = -1;
     cudaStream_t st = nullptr;
+    cudaStream_t side = nullptr;           // second branch of the loop graph (need dilation)
+    cudaEvent_t fork = nullptr, join = nullptr;
     cudaEvent_t ev[6] = {};
     cudaEvent_t prof[8] = {};              // kernel-group timing (opts.profile)
     void* base = nullptr;
@@ -317,6 +319,9 @@ Instance& instance() {
     Instance* I = new Instance();
     I->dev = dev;
     EGG_CHECK(cudaStreamCreateWithFlags(&I->st, cudaStreamNonBlocking));
+    EGG_CHECK(cudaStreamCreateWithFlags(&I->side, cudaStreamNonBlocking));
+    EGG_CHECK(cudaEventCreateWithFlags(&I->fork, cudaEventDisableTiming));
+    EGG_CHECK(cudaEventCreateWithFlags(&I->join, cudaEventDisableTiming));
     for (auto& e2 : I->ev) EGG_CHECK(cudaEventCreate(&e2));
     EGG_CHECK(cudaMallocHost((void**)&I->h_ctrl, kCtrlWords * sizeof(int)));
     g_inst[dev] = I;
@@ -431,8 +436,19 @@ void enqueue_part(Instance& I, int part, cudaGraphConditionalHandle h, int in_gr
     }
     mark(1);
     mark(2);
-    launch_cell_sums(single(I.g, I.w), st);
-    launch_need(single(I.g, I.w), st);
+    if (in_graph) {
+        // the need dilation reads only the dirty marks of the last update: a
+        // parallel branch of the graph beside the cell sums
+        EGG_CHECK(cudaEventRecord(I.fork, st));
+        EGG_CHECK(cudaStreamWaitEvent(I.side, I.fork, 0));
+        launch_need(single(I.g, I.w), I.side);
+        EGG_CHECK(cudaEventRecord(I.join, I.side));
+        launch_cell_sums(single(I.g, I.w), st);
+        EGG_CHECK(cudaStreamWaitEvent(st, I.join, 0));
+    } else {
+        launch_cell_sums(single(I.g, I.w), st);
+        launch_need(single(I.g, I.w), st);
+    }
     if (I.g.order_mode == 2 || I.g.stop_rule == 1) launch_order_param(I.g, I.w, -1, st);
     mark(3);
     mark(4);
@@ -1038,6 +1054,9 @@ int release() {
         for (auto e : I->prof)
             if (e) cudaEventDestroy(e);
         if (I->st) cudaStreamDestroy(I->st);
+        if (I->side) cudaStreamDestroy(I->side);
+        if (I->fork) cudaEventDestroy(I->fork);
+        if (I->join) cudaEventDestroy(I->join);
         cudaSetDevice(cur);
         delete I;
     }

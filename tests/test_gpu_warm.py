@@ -130,7 +130,11 @@ def test_trained_network_gain_over_plain():
     cases = [data.train_instance(1_600_000 + s) for s in range(2)] + [data.c5(0)]
     for c in cases:
         X, eps = c["X"], c["eps"]
-        egg_sync(X, eps)  # warm the workspace for this size
+        # one untimed call of each path first: workspaces and network buffers
+        # are allocated on first use (an earlier test may have released them)
+        egg_sync(X, eps)
+        egg_sync(X, eps, warm_start=m)
+        egg_sync(X, eps, warm_start=untrained)
         plain, pi = egg_sync(X, eps)
         lab, wi = egg_sync(X, eps, warm_start=m)
         lab_u, ui = egg_sync(X, eps, warm_start=untrained)
