@@ -318,7 +318,7 @@ struct Plan {
     int* d_boff_all = nullptr;
     int* d_active_all = nullptr;
     int* d_nact_all = nullptr;
-    int* d_loop = nullptr;
+    int* d_loop = nullptr;            // [2 + groups]: iterations, any active, sort openings per group
     int* d_results = nullptr;
     unsigned long long* d_loop_stamps = nullptr;
     float* d_in = nullptr;            // staged host inputs
@@ -432,19 +432,22 @@ void set_tables(Plan& P, const Config& c) {
     }
 }
 
-// one iteration of group k's instances; part 0 = up to the update, 1 = the
-// extra check (in the loop graph behind a conditional node), -1 = both
+// one iteration of group k's instances.  Parts, in order: 0 = grid check,
+// 1 = grid sort, 2 = cell sums, need, update, 3 = extra check; in the loop
+// graph parts 1 and 3 sit behind conditional nodes (gated: the extra
+// check's gate did the stage stamp and count).  -1 = all four, ungated.
 void enqueue_group(Plan& P, int k, cudaStream_t st, int part = -1) {
     Group& gr = P.groups[k];
     const Exec ex = batched(gr.act, gr.d);
-    if (part != 1) {
-        launch_build_check(ex, st, false);  // the control kernel cleared the changed words
-        launch_build_sort(ex, st);
+    const bool all = part < 0;
+    if (all || part == 0) launch_build_check(ex, st, false);  // the control kernel cleared the changed words
+    if (all || part == 1) launch_build_sort(ex, st);
+    if (all || part == 2) {
         launch_cell_sums(ex, st);
         launch_need(ex, st);
         launch_update(ex, nullptr, st);
     }
-    if (part != 0) launch_extra_check(ex, st, part == 1);
+    if (all || part == 3) launch_extra_check(ex, st, part == 3);
 }
 
 void enqueue_iteration(State& S, Plan& P, cudaGraphConditionalHandle h, int in_graph) {
@@ -531,50 +534,63 @@ cudaGraphExec_t get_graph(State& S, Plan& P, const Config& c) {
             cp.conditional.size = 1;
             e = cudaGraphAddNode(&ifs[k], body, &gate, 1, &cp);
             if (e != cudaSuccess) break;
-            // group body: [check .. update, gate] -> IF(some instance flagged) [extra check]
+            // group body: [check, gate] -> IF(some point changed cell) [sort] ->
+            // [cell sums .. update, gate] -> IF(some instance flagged) [extra check]
             cudaGraph_t gbody = cp.conditional.phGraph_out[0];
-            cudaGraphConditionalHandle hx;
-            e = cudaGraphConditionalHandleCreate(&hx, gbody, 0, 0);
-            if (e != cudaSuccess) break;
-            e = cudaStreamBeginCaptureToGraph(S.st, gbody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-            if (e != cudaSuccess) break;
+            const Exec gex = batched(P.groups[k].act, P.groups[k].d);
+            cudaGraphNode_t prev = nullptr;  // last node so far (nullptr: none)
             bool ok = true;
-            cudaGraphNode_t tail = nullptr;
-            try {
-                enqueue_group(P, k, S.st, 0);
-                launch_batch_gate_extra(batched(P.groups[k].act, P.groups[k].d), hx, S.st);
-                cudaStreamCaptureStatus cs;
-                const cudaGraphNode_t* deps = nullptr;
-                size_t nd = 0;
-                EGG_CHECK(cudaStreamGetCaptureInfo(S.st, &cs, nullptr, nullptr, &deps, &nd));
-                if (nd == 1) tail = deps[0];
-            } catch (const CudaError& ce) {
-                ok = false;
-                e = ce.code;
-            }
-            cudaGraph_t captured = nullptr;
-            const cudaError_t e2 = cudaStreamEndCapture(S.st, &captured);
-            if (ok) e = e2;
-            if (e == cudaSuccess && !tail) e = cudaErrorUnknown;
-            if (e != cudaSuccess) break;
-            cudaGraphNodeParams xp = {cudaGraphNodeTypeConditional};
-            xp.conditional.handle = hx;
-            xp.conditional.type = cudaGraphCondTypeIf;
-            xp.conditional.size = 1;
-            cudaGraphNode_t ifx;
-            e = cudaGraphAddNode(&ifx, gbody, &tail, 1, &xp);
-            if (e != cudaSuccess) break;
-            e = cudaStreamBeginCaptureToGraph(S.st, xp.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                              cudaStreamCaptureModeThreadLocal);
-            if (e != cudaSuccess) break;
-            try {
-                enqueue_group(P, k, S.st, 1);
-            } catch (const CudaError& ce) {
-                ok = false;
-                e = ce.code;
-            }
-            const cudaError_t e3 = cudaStreamEndCapture(S.st, &captured);
-            if (ok) e = e3;
+            // capture `fn` into graph `into` after the dependency `dep`; its last node -> *last
+            auto seg = [&](cudaGraph_t into, cudaGraphNode_t dep, cudaGraphNode_t* last, auto&& fn) {
+                cudaError_t r = cudaStreamBeginCaptureToGraph(S.st, into, dep ? &dep : nullptr, nullptr, dep ? 1 : 0,
+                                                              cudaStreamCaptureModeThreadLocal);
+                if (r != cudaSuccess) return r;
+                try {
+                    fn();
+                    if (last) {
+                        cudaStreamCaptureStatus cs;
+                        const cudaGraphNode_t* deps = nullptr;
+                        size_t nd = 0;
+                        EGG_CHECK(cudaStreamGetCaptureInfo(S.st, &cs, nullptr, nullptr, &deps, &nd));
+                        *last = nd == 1 ? deps[0] : nullptr;
+                    }
+                } catch (const CudaError& ce) {
+                    ok = false;
+                    r = ce.code;
+                }
+                cudaGraph_t captured = nullptr;
+                const cudaError_t r2 = cudaStreamEndCapture(S.st, &captured);
+                if (r == cudaSuccess) r = r2;
+                if (r == cudaSuccess && last && !*last) r = cudaErrorUnknown;
+                return r;
+            };
+            // an IF node after `dep` whose body is `fn`; the node -> *node
+            auto cond = [&](cudaGraphConditionalHandle hc, cudaGraphNode_t dep, cudaGraphNode_t* node, auto&& fn) {
+                cudaGraphNodeParams xp = {cudaGraphNodeTypeConditional};
+                xp.conditional.handle = hc;
+                xp.conditional.type = cudaGraphCondTypeIf;
+                xp.conditional.size = 1;
+                cudaError_t r = cudaGraphAddNode(node, gbody, &dep, 1, &xp);
+                if (r == cudaSuccess) r = seg(xp.conditional.phGraph_out[0], nullptr, nullptr, fn);
+                return r;
+            };
+            cudaGraphConditionalHandle hsort, hx;
+            e = cudaGraphConditionalHandleCreate(&hsort, gbody, 0, 0);
+            if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hx, gbody, 0, 0);
+            if (e == cudaSuccess)
+                e = seg(gbody, nullptr, &prev, [&] {
+                    enqueue_group(P, k, S.st, 0);
+                    launch_batch_gate_sort(gex, hsort, P.d_loop + 2 + k, S.st);
+                });
+            cudaGraphNode_t ifs_sort = nullptr, ifs_x = nullptr;
+            if (e == cudaSuccess) e = cond(hsort, prev, &ifs_sort, [&] { enqueue_group(P, k, S.st, 1); });
+            if (e == cudaSuccess)
+                e = seg(gbody, ifs_sort, &prev, [&] {
+                    enqueue_group(P, k, S.st, 2);
+                    launch_batch_gate_extra(gex, hx, S.st);
+                });
+            if (e == cudaSuccess) e = cond(hx, prev, &ifs_x, [&] { enqueue_group(P, k, S.st, 3); });
+            if (!ok && e == cudaSuccess) e = cudaErrorUnknown;
         }
         if (e == cudaSuccess) {
             CtlArgs a = ctl_args(P);
@@ -697,7 +713,7 @@ void make_plan(State& S, Plan& P, egg_batch_item* items, int count, const egg_op
     const size_t o_boff_all = reserve(4 * tab);
     const size_t o_act_all = reserve(4 * (size_t)G * P.cap);
     const size_t o_nact_all = reserve(4 * G);
-    const size_t o_loop = reserve(4 * 2);
+    const size_t o_loop = reserve(4 * (2 + (size_t)G));
     const size_t o_res = reserve(4 * 5 * (size_t)count);
     const size_t o_ls = reserve(8 * ((size_t)P.max_iter + 2));
     const size_t o_in = reserve(4 * P.in_floats);
@@ -790,27 +806,32 @@ int enqueue_prologue(State& S, Plan& P, int max_iter) {
         kb_load<<<ex.blocks(kShapeCapN256L, 256), 256, 0, S.st>>>(ex.args(kShapeCapN256L));
         launches++;
     }
-    EGG_CHECK(cudaMemsetAsync(P.d_loop, 0, 8, S.st));
+    EGG_CHECK(cudaMemsetAsync(P.d_loop, 0, 4 * (2 + P.groups.size()), S.st));
     k_batch_ctl<<<1, 1024, 0, S.st>>>(ctl_args(P), 0, 0, 0);
     return launches + 1;
 }
 
-// kernels of one group's iteration: build (grid check, radix passes, 4
+// kernels of one group's iteration: grid check, sort (radix passes, 4
 // tables), cell sums (2), need, update, extra check (3)
-int group_launches(const Group& gr) { return 1 + 3 * gr.act.max_passes + 4 + 2 + 1 + 1 + 3; }
+int sort_launches(const Group& gr) { return 3 * gr.act.max_passes + 4; }
+int group_launches(const Group& gr) { return 1 + sort_launches(gr) + 2 + 1 + 1 + 3; }
 
 // Kernels of the loop graph: gate and control every iteration, and each
 // group's kernels in the iterations where it had active instances (the
 // largest iteration count among its instances; an idle group's conditional
-// node launches nothing): the extra-check gate every such iteration, the
-// three extra-check kernels only where an instance's flag reached it
-// (counted once per instance: its final iteration).
+// node launches nothing): the two gates every such iteration, the sort
+// where its gate opened (counted on the device), the three extra-check
+// kernels only where an instance's flag reached it (counted once per
+// instance: its final iteration).
 long long loop_launches(const Plan& P, int loop_iters, const std::vector<int>& res) {
     long long l = 2LL * loop_iters;
-    for (const Group& gr : P.groups) {
+    const int* opened = res.data() + 5 * (size_t)P.count + 2;
+    for (size_t k = 0; k < P.groups.size(); k++) {
+        const Group& gr = P.groups[k];
         int m = 0;
         for (int pos = gr.begin; pos < gr.end; pos++) m = std::max(m, res[5 * (size_t)pos]);
-        l += (long long)m * (group_launches(gr) - 3 + 1) + 3LL * (gr.end - gr.begin);
+        l += (long long)m * (group_launches(gr) - 3 - sort_launches(gr) + 2) +
+             (long long)opened[k] * sort_launches(gr) + 3LL * (gr.end - gr.begin);
     }
     return l;
 }
@@ -953,9 +974,10 @@ int run_batch(egg_batch_item* items, int count, const egg_opts* opts_in, egg_bat
     launches++;
     const size_t out_b = 4 * P.out_ints;
     if (out_b) EGG_CHECK(cudaMemcpyAsync(S.h_pinned, P.d_out, out_b, cudaMemcpyDeviceToHost, S.st));
-    std::vector<int> res(5 * (size_t)count + 2);
+    const size_t nloop = 2 + P.groups.size();
+    std::vector<int> res(5 * (size_t)count + nloop);
     EGG_CHECK(cudaMemcpyAsync(res.data(), P.d_results, 4 * 5 * (size_t)count, cudaMemcpyDeviceToHost, S.st));
-    EGG_CHECK(cudaMemcpyAsync(res.data() + 5 * (size_t)count, P.d_loop, 8, cudaMemcpyDeviceToHost, S.st));
+    EGG_CHECK(cudaMemcpyAsync(res.data() + 5 * (size_t)count, P.d_loop, 4 * nloop, cudaMemcpyDeviceToHost, S.st));
     EGG_CHECK(cudaEventRecord(S.ev[3], S.st));
     EGG_CHECK(cudaStreamSynchronize(S.st));
     EGG_CHECK(cudaGetLastError());
@@ -987,7 +1009,8 @@ int run_batch(egg_batch_item* items, int count, const egg_opts* opts_in, egg_bat
         stats->loop_iterations = loop_iters;
         stats->groups = (int)P.groups.size();
         long long ll = loop_launches(P, loop_iters, res);
-        if (!graph_loop) {  // host-driven loop: every group launches in every iteration, no gate
+        if (!graph_loop || (int)P.groups.size() > kMaxGroups) {
+            // host-driven loop, or a graph without gates: every group launches in every iteration
             ll = loop_iters;
             for (const Group& gr : P.groups) ll += (long long)loop_iters * group_launches(gr);
         }

@@ -308,6 +308,26 @@ void launch_batch_gate_extra(const Exec& ex, cudaGraphConditionalHandle h, cudaS
     k_batch_gate_extra<<<1, 1024, 0, st>>>(ex.bt->works, ex.bt->active, ex.bt->nact, h);
 }
 
+// Opens the grid-sort node of one dimension group when the grid check found
+// a point that left its cell in any of the group's active instances (for
+// the others the sort kernels would return at once); counts the openings.
+__global__ void __launch_bounds__(1024) k_batch_gate_sort(const Work* __restrict__ works,
+                                                          const int* __restrict__ active, const int* __restrict__ nact,
+                                                          int* __restrict__ opened, cudaGraphConditionalHandle h) {
+    const int na = *nact;
+    int changed = 0;
+    for (int t = threadIdx.x; t < na; t += blockDim.x) changed |= works[active[t]].ctrl[kCtrlChanged] != 0;
+    const int any = __syncthreads_or(changed);
+    if (threadIdx.x == 0) {
+        if (any) *opened += 1;
+        cudaGraphSetConditional(h, any ? 1u : 0u);
+    }
+}
+
+void launch_batch_gate_sort(const Exec& ex, cudaGraphConditionalHandle h, int* opened, cudaStream_t st) {
+    k_batch_gate_sort<<<1, 1024, 0, st>>>(ex.bt->works, ex.bt->active, ex.bt->nact, opened, h);
+}
+
 // The kernels return at once unless the update left the flag at 1; the
 // grids are bounded so that the common early exit costs little.  gated: the
 // call sits behind k_gate_extra, which did the stage stamp and the count.

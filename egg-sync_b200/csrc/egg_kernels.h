@@ -100,5 +100,8 @@ void launch_extra_check(const Exec& ex, cudaStream_t st, bool gated = false);
 void launch_gate_extra(const Work& w, cudaGraphConditionalHandle h, cudaStream_t st);
 // loop graph of a batch: the same per dimension group (any active instance flagged)
 void launch_batch_gate_extra(const Exec& ex, cudaGraphConditionalHandle h, cudaStream_t st);
+// ... and its grid sort (any active instance with a point that changed cell;
+// *opened counts the openings)
+void launch_batch_gate_sort(const Exec& ex, cudaGraphConditionalHandle h, int* opened, cudaStream_t st);
 
 }  // namespace egg
