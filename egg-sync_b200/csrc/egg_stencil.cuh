@@ -7,9 +7,14 @@
 // in exact and rounded arithmetic alike (their gap exceeds (r+1)*side > eps).
 //
 // Must be called by all 32 lanes of a warp.  When every lane has the same
-// outer cell, the warp resolves the stencil entries in parallel (lane =
-// entry) and visits each candidate cell with all lanes in lockstep (the cell
-// records become broadcast loads); otherwise each lane walks its own stencil.
+// outer cell and their cells in dimension od lie within kLockZSpan of each
+// other, the warp resolves the stencil entries in parallel (lane = entry)
+// and visits each candidate cell with all lanes in lockstep (the cell
+// records become broadcast loads); otherwise each lane walks its own stencil
+// (the lockstep window in dimension od is the union of the lanes' windows, so
+// lanes spread along od would each test many cells that only others need).
+// Both paths give every lane the same results bit for bit: the extra cells
+// of the union fail that lane's box test.
 // fn(c) is called once per candidate cell per lane, in increasing stencil
 // entry then increasing cell order in both paths.  A lane for which
 // active() is false needs no result: it rides along in the lockstep path
@@ -27,6 +32,10 @@
 
 namespace egg {
 
+// warps whose cells in dimension od span more than this take the per-lane walk
+// (1M x 3D: 96.4 -> 95.5 ms against lockstep for every single-column warp)
+constexpr int kLockZSpan = 4;
+
 // colmask bits of the blocks meeting the cells [zl, zh] of dimension od
 __device__ __forceinline__ unsigned long long zwindow_mask(const Geom& g, int zl, int zh) {
     const int bl = max(0, zl) / g.zblk, bh = min(g.width - 1, zh) / g.zblk;
@@ -38,16 +47,16 @@ __device__ __forceinline__ void for_candidates(const Geom& g, const Work& w, con
                                                int d, A&& active, F&& fn) {
     const int nst = w.st_count[0];
     const int ob0 = __shfl_sync(0xffffffffu, obase, 0);
-    if (__all_sync(0xffffffffu, obase == ob0)) {
-        int zlo = 0, zhi = 0;
-        if (g.od < d) {
-            zlo = zhi = gi[g.od];
+    int zlo = 0, zhi = 0;
+    if (g.od < d) {
+        zlo = zhi = gi[g.od];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                zlo = min(zlo, __shfl_xor_sync(0xffffffffu, zlo, o));
-                zhi = max(zhi, __shfl_xor_sync(0xffffffffu, zhi, o));
-            }
+        for (int o = 16; o > 0; o >>= 1) {
+            zlo = min(zlo, __shfl_xor_sync(0xffffffffu, zlo, o));
+            zhi = max(zhi, __shfl_xor_sync(0xffffffffu, zhi, o));
         }
+    }
+    if (__all_sync(0xffffffffu, obase == ob0) && zhi - zlo <= kLockZSpan) {
         for (int s0 = 0; s0 < nst; s0 += 32) {
             const int s = s0 + lane;
             int cb = 0, ce = 0;
