@@ -122,6 +122,7 @@ struct Work {
     unsigned long long* need;      // [n_outer]
     unsigned char* viol_orig;  // [ns] by original index
     unsigned char* warp_moved; // [ns/32 + 1] the warp's points changed in the last update (grid check)
+    unsigned* warp_viol;       // [ns/32 + 1] the warp's violation bits (lane mask) as of its last update
     int* span_list;            // [ns/32 + 1] cells whose points span 2-3 warps
     int* big_list;             // [ns/128 + 1] cells whose points span 4 or more warps
     int* span_mark;            // [ns] per spanning cell: the last iteration that re-summed one of its warps

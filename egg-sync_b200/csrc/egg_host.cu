@@ -198,6 +198,7 @@ size_t layout_work(const Geom& g, int max_iter, char* base, Work& w, float** xin
     add((void**)&w.need, 8 * ((size_t)g.n_outer + 1));
     add((void**)&w.viol_orig, ns);
     add((void**)&w.warp_moved, (size_t)nw + 1);
+    add((void**)&w.warp_viol, 4 * ((size_t)nw + 1));
     add((void**)&w.span_list, 4 * ((size_t)nw + 1));
     add((void**)&w.big_list, 4 * ((size_t)nw / 4 + 1));
     add((void**)&w.span_mark, 4 * ns);
@@ -752,23 +753,24 @@ int run(const float* x, int64_t n, int32_t d, float eps, float lam, const egg_op
             stats->kernel_launches[k] = kl[k];
         }
         // launches: reset + transpose; per iteration: begin, grid check,
-        // grid sort (3 per radix pass + 4), 2 cell sums, need, [2 order
-        // parameter], update, 3 extra check, end; then the final build
-        // (begin, check, sort), labels (1 or 4 kernels), [2 cell sums + 2
-        // order parameter], [positions].  In the loop graph two gate kernels
-        // run every iteration, the grid sort only in iterations where some
-        // point changed cell and the extra check only where the update left
-        // the flag at 1.
-        const int sort_l = 3 * plan_count(g) + 4;
+        // grid sort (3 per radix pass + 4; with one 32-bit key, 1 + 3 per
+        // pass + 4), 2 cell sums, need, [2 order parameter], update, 3 extra
+        // check, end; then the final build (begin, check, sort), labels (1
+        // or 4 kernels), [2 cell sums + 2 order parameter], [positions].  In
+        // the loop graph two gate kernels run every iteration, the grid sort
+        // only in iterations where some point changed cell and the extra
+        // check only where the update left the flag at 1.
+        const bool onekey = I.w.skey[0] != nullptr && g.d <= 3 && g.width <= 256;
+        const int sort_l = onekey ? 3 * (1 + g.d) + 5 : 3 * plan_count(g) + 4;
         const int build_l = sort_l + 2;
-        const int per_iter = sort_l + 1 + 9 + ((g.order_mode == 2 || g.stop_rule == 1) ? 2 : 0);
+        const int order_l = (g.order_mode == 2 || g.stop_rule == 1) ? 2 : 0;
         const int final_l = build_l + (opts.labels_mode == 1 ? 1 : 4) + (g.order_mode == 1 ? 4 : 0) +
                             (opts.positions_out ? 1 : 0);
-        long long loop_l = (long long)iters * per_iter;
+        long long loop_l = (long long)iters * (sort_l + 10 + order_l);
         if (use_graph) {
             // grid builds in the loop: all builds but the final one when it rebuilt
             const int loop_builds = I.h_ctrl[kCtrlBuilds] - (I.h_ctrl[kCtrlChanged] ? 1 : 0);
-            loop_l = (long long)iters * (per_iter - sort_l - 1) + 3LL * I.h_ctrl[kCtrlExtraRuns] +
+            loop_l = (long long)iters * (9 + order_l) + 3LL * I.h_ctrl[kCtrlExtraRuns] +
                      (long long)loop_builds * sort_l;
         }
         stats->launches = (int32_t)(2 + loop_l + final_l + (opts.warm_start ? 10 : 0));

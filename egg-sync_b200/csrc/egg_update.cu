@@ -281,27 +281,31 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
     const int d = D > 0 ? D : g.d;
     extern __shared__ float s_tab[];
     const int K = g.table_k, TW = 2 * K + 1;
+    const int i = bx * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const bool valid = i < g.n;
+    const int iv = valid ? i : g.n - 1;  // lanes past n shadow the last point; their results are dropped
+    // the point and its warp's last violation bits are loaded before the
+    // table's barrier, so their latency overlaps it (most warps late in a
+    // run need nothing else)
+    float x[DM];
+    for (int l = 0; l < d; l++) x[l] = w.X[(size_t)l * g.ns + iv];
+    const unsigned wv_last = (w.warp_viol && (i & ~31) < g.n) ? w.warp_viol[i >> 5] : 0u;
     for (int t = threadIdx.x; t < 3 * TW; t += blockDim.x) s_tab[t] = w.table[t];
     if (bx == 0 && threadIdx.x == 0) {
         const int it = w.ctrl[kCtrlIter];
         w.stamps[4 * it + 1] = globaltimer();
     }
     __syncthreads();
-    const int i = bx * blockDim.x + threadIdx.x;
     if ((i & ~31) >= g.n) return;  // whole warp beyond n
-    const int lane = threadIdx.x & 31;
-    const bool valid = i < g.n;
-    const int iv = valid ? i : g.n - 1;  // lanes past n shadow the last point; their results are dropped
     const float* Ts = s_tab;
     const float* Tc = s_tab + TW;
     const float* Tm = s_tab + 2 * TW;
 
     const int it = w.ctrl[kCtrlIter];
-    float x[DM];
     int gi[DM];
     int obase = 0;
     for (int l = 0; l < d; l++) {
-        x[l] = w.X[(size_t)l * g.ns + iv];
         gi[l] = cell_dim(x[l], g);
         if (l < g.od) obase += gi[l] * g.wpow[l];
     }
@@ -316,17 +320,26 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
     // copied Xn into X; a rebuild reorders X only): a kept position is
     // written back only after a rebuild (the control word is read where it
     // is used, so nothing extra stays live over the walk)
+    // Without a rebuild the warp holds the same points as at its last update
+    // and its violation bits stand; a rebuild reorders the points, so the
+    // bits are gathered by original index and the warp's word rewritten.
     if (!__any_sync(0xffffffffu, need_me)) {
-        bool viol = false;
-        if (valid) {
-            if (w.ctrl[kCtrlChanged] != 0)
+        unsigned vb = wv_last;
+        if (w.ctrl[kCtrlChanged] != 0 || !w.warp_viol) {
+            bool viol = false;
+            if (valid) {
                 for (int l = 0; l < d; l++) w.Xn[(size_t)l * g.ns + i] = x[l];
-            viol = w.viol_orig[w.orig[i]] != 0;
+                viol = w.viol_orig[w.orig[i]] != 0;
+            }
+            vb = __ballot_sync(0xffffffffu, viol);
+            if (lane == 0 && w.warp_viol) w.warp_viol[i >> 5] = vb;
         }
-        if (lane == 0 && w.warp_moved) w.warp_moved[i >> 5] = 0;
-        if (__any_sync(0xffffffffu, viol) && lane == 0) {
-            volatile int* f = w.ctrl + kCtrlFlag;
-            if (*f != 0) *f = 0;
+        if (lane == 0) {
+            if (w.warp_moved) w.warp_moved[i >> 5] = 0;
+            if (vb != 0) {
+                volatile int* f = w.ctrl + kCtrlFlag;
+                if (*f != 0) *f = 0;
+            }
         }
         return;
     }
@@ -419,7 +432,8 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
     // so a border point with neighbours in a partial cell always violates.
     bool viol = false;
     if (valid && !walk) {
-        viol = w.viol_orig[w.orig[i]] != 0;
+        viol = (w.ctrl[kCtrlChanged] != 0 || !w.warp_viol) ? w.viol_orig[w.orig[i]] != 0
+                                                           : ((w.warp_viol[i >> 5] >> lane) & 1u) != 0;
     } else if (valid) {
         if (!border) viol = (N != own_cnt);
         else if (a.partial_in > 0) viol = true;
@@ -438,9 +452,13 @@ __device__ __forceinline__ void update_body(const Geom& g, const Work& w, int* _
     // the warps whose points moved: the next grid check reads only those
     const bool warp_mv = __any_sync(0xffffffffu, moved);
     if (lane == 0 && w.warp_moved) w.warp_moved[i >> 5] = warp_mv ? 1 : 0;
-    if (__any_sync(0xffffffffu, viol) && lane == 0) {
-        volatile int* f = w.ctrl + kCtrlFlag;
-        if (*f != 0) *f = 0;
+    const unsigned vb = __ballot_sync(0xffffffffu, viol);
+    if (lane == 0) {
+        if (w.warp_viol) w.warp_viol[i >> 5] = vb;
+        if (vb != 0) {
+            volatile int* f = w.ctrl + kCtrlFlag;
+            if (*f != 0) *f = 0;
+        }
     }
     if (a.tab_err) atomicOr(w.ctrl + kCtrlStatus, kErrTable);
 #ifdef EGG_UPDATE_STATS
