@@ -95,6 +95,17 @@ __device__ bool mbr_exact(const Geom& g, const Work& w, int qi, const float* xp)
 
 }  // namespace
 
+// Every point of cell c has the same coordinates (its tight box is a
+// point): they take the same steps in each kernel of the check, so one of
+// them (the cell's first) stands for all.  Near convergence nearly every
+// cell is such a collapsed cluster (1M x 3D: 41,646 of 41,660 final cells,
+// holding all but 44 points).
+__device__ __forceinline__ bool cell_degenerate(const Geom& g, const Work& w, int c, int d) {
+    for (int l = 0; l < d; l++)
+        if (__ldg(w.cbmin + (size_t)l * g.ns + c) != __ldg(w.cbmax + (size_t)l * g.ns + c)) return false;
+    return true;
+}
+
 // extremes of each point's eps/2 group (itself included)
 template <int D>
 __device__ __forceinline__ void ball_bbox_body(const Geom& g, const Work& w, int bx, int gx, int mark = 1) {
@@ -109,6 +120,9 @@ __device__ __forceinline__ void ball_bbox_body(const Geom& g, const Work& w, int
     }
     if (w.ctrl[kCtrlFlag] == 0) return;
     for (int i = bx * blockDim.x + threadIdx.x; i < g.n; i += gx * blockDim.x) {
+        // in a collapsed cell only the first point's extremes are read
+        const int ci = w.cell_of[i];
+        if (i != w.cell_start[ci] && cell_degenerate(g, w, ci, d)) continue;
         float xq[DM], lo[DM], hi[DM];
         int gq[DM];
         int obase = 0;
@@ -156,20 +170,38 @@ __device__ __forceinline__ void ball_bbox_body(const Geom& g, const Work& w, int
 
 // Union over a cell's points of their eps/2-group extremes.  The MBR of any
 // pair (p, q) with q in the cell lies inside it, so its distance to p is a
-// lower bound for every pair of the cell.
+// lower bound for every pair of the cell.  One warp per cell (collapsed
+// clusters hold tens of thousands of points); min and max do not depend on
+// the order of their operands, so the result is the serial one.
 __device__ __forceinline__ void cell_ballbox_body(const Geom& g, const Work& w, int bx, int gx) {
     if (w.ctrl[kCtrlFlag] == 0) return;
     const int M = w.ctrl[kCtrlM];
-    for (int c = bx * blockDim.x + threadIdx.x; c < M; c += gx * blockDim.x) {
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    for (int c = bx * wpb + (threadIdx.x >> 5); c < M; c += gx * wpb) {
         const int qb = w.cell_start[c], qe = w.cell_start[c + 1];
+        const bool deg = cell_degenerate(g, w, c, g.d);
         for (int l = 0; l < g.d; l++) {
-            float lo = 3.0e38f, hi = -3.0e38f;
-            for (int q = qb; q < qe; q++) {
-                lo = fminf(lo, w.qlo[(size_t)l * g.ns + q]);
-                hi = fmaxf(hi, w.qhi[(size_t)l * g.ns + q]);
+            float lo, hi;
+            if (deg) {
+                lo = w.qlo[(size_t)l * g.ns + qb];
+                hi = w.qhi[(size_t)l * g.ns + qb];
+            } else {
+                lo = 3.0e38f;
+                hi = -3.0e38f;
+                for (int q = qb + lane; q < qe; q += 32) {
+                    lo = fminf(lo, w.qlo[(size_t)l * g.ns + q]);
+                    hi = fmaxf(hi, w.qhi[(size_t)l * g.ns + q]);
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+                    hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+                }
             }
-            w.ulo[(size_t)l * g.ns + c] = lo;
-            w.uhi[(size_t)l * g.ns + c] = hi;
+            if (lane == 0) {
+                w.ulo[(size_t)l * g.ns + c] = lo;
+                w.uhi[(size_t)l * g.ns + c] = hi;
+            }
         }
     }
 }
@@ -182,6 +214,12 @@ __device__ __forceinline__ void annulus_body(const Geom& g, const Work& w, int b
     if (*flag == 0) return;
     int pairs = 0;
     for (int i = bx * blockDim.x + threadIdx.x; i < g.n; i += gx * blockDim.x) {
+        // a point of a collapsed cell finds what the cell's first point finds
+        const int cp = w.cell_of[i];
+        const int pb = w.cell_start[cp];
+        const bool pdeg = cell_degenerate(g, w, cp, d);
+        if (pdeg && i != pb) continue;
+        const int pw = pdeg ? w.cell_start[cp + 1] - pb : 1;  // points it stands for (pair count)
         float xp[DM];
         int gp[DM];
         int obase = 0;
@@ -206,11 +244,14 @@ __device__ __forceinline__ void annulus_body(const Geom& g, const Work& w, int b
             tight_box_dist2(xp, w.ulo + c, w.uhi + c, g.ns, d, lb2, ub2);
             if (lb2 > g.t_eps) return true;  // no pair of this cell can have its MBR within eps
             const int qb = __ldg(w.cell_start + c), qe = __ldg(w.cell_start + c + 1);
-            for (int q = qb; q < qe; q++) {
+            // a collapsed cell: its first point decides for all of them
+            const bool qdeg = cell_degenerate(g, w, c, d);
+            const int qend = qdeg ? qb + 1 : qe;
+            for (int q = qb; q < qend; q++) {
                 float d2 = 0.f;
                 for (int l = 0; l < d; l++) d2 = dist_step(xp[l], __ldg(w.X + (size_t)l * g.ns + q), d2);
                 if (!(d2 > g.t_eps && d2 <= g.t_extra)) continue;
-                pairs++;
+                pairs += pw * (qdeg ? qe - qb : 1);
                 bool resolved = true;
                 float acc = 0.f;
                 for (int l = 0; l < d; l++) {

@@ -3,11 +3,13 @@
 // The reference labels a point with the compacted index of its final cell
 // when that cell holds more than one point, else -1
 // (src/algorithms/EGG_SynC.cu:1205-1227, 1504-1522).  Here the collapsed
-// points are joined into components by a lock-free union-find: every pair of
-// consecutive cell-sorted points in the same final cell is an edge; a link
-// hooks the larger root onto the smaller one with atomicCAS, so every
-// component's root is its smallest sorted index, i.e. the first point of the
-// cell, whatever the order of the atomics.  After full path compression a
+// points are joined into components by a lock-free union-find: every point
+// is joined to the first cell-sorted point of its final cell (a star per
+// cell: one hook per point, where a chain of consecutive points made finds
+// walk paths as long as the cluster); a link hooks the larger root onto the
+// smaller one with atomicCAS, so every component's root is its smallest
+// sorted index, i.e. the first point of the cell, whatever the order of the
+// atomics.  Component sizes are counted with one atomic per warp and root.  After full path compression a
 // point's label is the cell index of its root when the component holds more
 // than one point: the reference's partition and label values, deterministic.
 #include "egg_common.cuh"
@@ -52,16 +54,20 @@ __device__ __forceinline__ void uf_init_body(const Geom& g, const Work& w, int b
     }
 }
 
-// edge (i, i+1) whenever both points lie in the same final cell
+// edge (first point of i's final cell, i)
 __device__ __forceinline__ void uf_link_body(const Geom& g, const Work& w, int bx, int gx) {
-    for (int i = bx * blockDim.x + threadIdx.x; i + 1 < g.n; i += gx * blockDim.x)
-        if (w.cell_of[i] == w.cell_of[i + 1]) uf_union(w.uf_parent, i, i + 1);
+    for (int i = bx * blockDim.x + threadIdx.x; i < g.n; i += gx * blockDim.x) {
+        const int f = w.cell_start[w.cell_of[i]];
+        if (f != i) uf_union(w.uf_parent, f, i);
+    }
 }
 
 __device__ __forceinline__ void uf_compress_body(const Geom& g, const Work& w, int bx, int gx) {
     for (int i = bx * blockDim.x + threadIdx.x; i < g.n; i += gx * blockDim.x) {
         const int r = uf_find(w.uf_parent, i);
-        atomicAdd(w.uf_size + r, 1);
+        // lanes with the same root add once (sorted points share roots)
+        const unsigned peers = __match_any_sync(__activemask(), r);
+        if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(w.uf_size + r, __popc(peers));
     }
 }
 
