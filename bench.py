@@ -80,6 +80,9 @@ def parse():
     ap.add_argument("--sync-iterations", action="store_true",
                     help="count the reference CPU SynC's iterations on the workload (brute-force GPU SynC)")
     ap.add_argument("--sync-max-iter", type=int, default=300)
+    ap.add_argument("--stage-split", action="store_true",
+                    help="per-phase split of the loop graph's time (iterations 0-11, 12-59, 60+) from the "
+                         "per-iteration %%globaltimer stamps, and the slowest iterations")
     ap.add_argument("--profile-grid", action="store_true",
                     help="for ncu: six grid builds of the workload from device-resident points (L2 flushed "
                          "before each), no timing")
@@ -101,6 +104,46 @@ def profile_run(args):
     torch.cuda.synchronize(dev)
     print(json.dumps({"profile_run": True, "n": len(c["X"]), "iterations": info["iterations"],
                       "launches_per_run": info["launches"]}))
+
+
+def stage_split(args):
+    """Where the loop graph's time goes by phase of the run, on the device's
+    own clock: each iteration stamps its start, the update's start, the end
+    of the update (the extra-check gate) and its end; runs stopped after 12
+    and 60 iterations follow the full run's trajectory exactly, so the
+    differences of the stage sums give each phase (median of 4 runs each)."""
+    import numpy as np
+    import torch
+
+    from eggsync import data, egg_sync
+
+    dev = torch.device("cuda", 0)
+    c = data.c5(args.seed, n=args.n)
+    Xd = torch.from_numpy(c["X"]).to(dev)
+    lab = torch.empty(len(c["X"]), dtype=torch.int32, device=dev)
+
+    def runs(k):
+        rows, info = [], None
+        for r in range(5):
+            _, info = egg_sync(Xd, c["eps"], labels_out=lab, max_iter=k)
+            rows.append(info["stage_ms"][1:4] + [info["grid_builds"], info["extra_checks"], info["total_ms"]])
+        return np.median(np.array(rows[1:]), 0), info
+
+    s12, _ = runs(12)
+    s60, _ = runs(60)
+    sall, info = runs(0)
+    iters = info["iterations"]
+    out = {"workload": "1M x 3D (c5 shape), eps %.3f" % c["eps"], "iterations": iters, "total_ms": sall[5],
+           "columns": ["before the update (grid check, sort, cell sums, need)", "update",
+                       "update end to iteration end (extra check when it runs)"]}
+    for name, hi, lo, n_it in (("0-11", s12, None, 12), ("12-59", s60, s12, 48), ("60+", sall, s60, iters - 60)):
+        dlt = hi if lo is None else hi - lo
+        out[name] = {"ms": [round(float(v), 3) for v in dlt[:3]], "us_per_iteration": [
+            round(float(v) * 1e3 / n_it, 1) for v in dlt[:3]], "grid_builds": int(dlt[3]), "extra_checks": int(dlt[4])}
+    itr = np.array(info["itr_ms"])
+    top = np.argsort(-itr)[:5]
+    out["slowest_iterations_ms"] = {int(k): round(float(itr[k]), 3) for k in top}
+    print(json.dumps(out))
 
 
 def profile_grid(args):
@@ -679,6 +722,9 @@ def main():
         return
     if args.profile_grid:
         profile_grid(args)
+        return
+    if args.stage_split:
+        stage_split(args)
         return
     if args.sync_iterations:
         sync_iterations(args)
