@@ -11,10 +11,11 @@
 //              64-bit fixed-point sums (integer atomics: the result does not
 //              depend on the order of the additions), then one row of
 //              feat_dim(d) values per point (192 for d = 3).
-//   inference  k_mlp_infer: the three layers fused in one kernel on the
-//              tensor cores (BF16 operands, FP32 accumulation, mma.sync
-//              m16n8k16); a warp owns 16 points, a layer's accumulators stay
-//              in registers and become the next layer's operand fragments.
+//   inference  k_mlp_infer_tc: the three layers fused in one kernel on the
+//              5th-generation tensor cores (tcgen05.mma, BF16 operands from
+//              shared memory, FP32 accumulators in TMEM); a CTA owns
+//              128-point tiles, the next tile's features arrive by cp.async
+//              while the current one runs.
 //   training   FP32 kernels: tiled SGEMM, bias/ReLU, ReLU backward, column
 //              sums (fixed order), MSE gradient, Adam.  The gradient of one
 //              batch is exported (egg_mlp_grad) so that tests can check it
@@ -147,15 +148,6 @@ __global__ void k_features(FGrid G, const float* __restrict__ X, size_t sp, size
 // ---------------------------------------------------------------------------
 // inference: fused 3-layer MLP on the tensor cores
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void mma_bf16(float (&c)[4], unsigned a0, unsigned a1, unsigned a2, unsigned a3,
-                                         unsigned b0, unsigned b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};\n"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-}
-
 __device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
     __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
     return *reinterpret_cast<unsigned*>(&v);
@@ -175,99 +167,246 @@ struct Packed {
     int dout;
 };
 
-constexpr int kInferWarps = 4;
+// ---------------------------------------------------------------------------
+// inference on the 5th-generation tensor cores (tcgen05, TMEM accumulators)
+// ---------------------------------------------------------------------------
+// A CTA of four warps owns 128-point tiles (the MMA's M).  The three layers
+// run as chains of tcgen05.mma (K = 16 per instruction, BF16 operands from
+// shared memory, FP32 accumulation in 128 TMEM columns) issued by one
+// thread and committed to an mbarrier; after each layer every warp reads its
+// 32 TMEM lanes (rows) with tcgen05.ld, adds the bias, applies the ReLU and
+// writes the rounded BF16 row as the next layer's A operand.  Operands use
+// the no-swizzle K-major layout: a core matrix of 8 rows x 8 elements is 128
+// contiguous bytes, the core matrices of one 8-element chunk of K follow each
+// other down the rows (stride 128 bytes) and chunks are rows / 8 * 128 bytes
+// apart.  Each output row depends on its own features only (the MMA sums K
+// in the same order for every row), whatever the tile around it.
+namespace tc {
 
-__host__ __device__ inline int w1_stride(int fp) { return fp + 8; }
-constexpr int kW2Stride = kHidden + 8;
+constexpr int kRows = 128;     // points per tile
+constexpr int kThreads = 128;  // warp w reads TMEM lanes 32w .. 32w + 31
+constexpr int kN3 = 16;        // layer 3 padded to the smallest N of an M = 128 MMA
+constexpr int kCols = 128;     // TMEM columns (FP32 accumulators of 128 outputs)
+constexpr long kWaitLimit = 1L << 20;
 
-__host__ __device__ inline size_t infer_smem(int fp) {
-    return sizeof(__nv_bfloat16) * ((size_t)kHidden * w1_stride(fp) + (size_t)kHidden * kW2Stride + 8 * kW2Stride) +
-           sizeof(float) * (2 * kHidden + 8);
+__device__ __forceinline__ uint32_t cm_offset(int row, int kchunk, int rows) {
+    return (uint32_t)kchunk * (uint32_t)(rows / 8) * 128u + (uint32_t)(row >> 3) * 128u + (uint32_t)(row & 7) * 16u;
 }
 
-__global__ void __launch_bounds__(32 * kInferWarps) k_mlp_infer(Packed P, const __nv_bfloat16* __restrict__ feats,
-                                                                 int n, float* __restrict__ out) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int fp = P.fp, s1 = w1_stride(fp);
-    __nv_bfloat16* W1 = reinterpret_cast<__nv_bfloat16*>(smem);
-    __nv_bfloat16* W2 = W1 + (size_t)kHidden * s1;
-    __nv_bfloat16* W3 = W2 + (size_t)kHidden * kW2Stride;
-    float* B1 = reinterpret_cast<float*>(W3 + 8 * kW2Stride);
+// shared-memory matrix descriptor: start, leading (K) and stride (M/N) byte
+// offsets >> 4, descriptor version 1, no swizzle
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// instruction descriptor: F32 accumulator, BF16 A and B, both K-major, M = 128
+__device__ __forceinline__ uint32_t idesc_bf16(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kRows >> 4) << 24);
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// bounded wait for the mbarrier's phase; false when the limit ran out
+__device__ __forceinline__ bool wait_phase(uint32_t bar, uint32_t phase) {
+    for (long it = 0; it < kWaitLimit; it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__host__ inline size_t smem_bytes(int fp) {
+    const size_t ka = (size_t)std::max(fp, kHidden);
+    return 1024 + 2 * ((size_t)kHidden * fp + (size_t)kHidden * kHidden + (size_t)kN3 * kHidden + 2 * (size_t)kRows * ka) +
+           4 * (2 * kHidden + kN3) + 16;
+}
+
+}  // namespace tc
+
+// status: set to 1 (and the tile's outputs to NaN) if an MMA never completed
+__global__ void __launch_bounds__(tc::kThreads, 1) k_mlp_infer_tc(Packed P, const __nv_bfloat16* __restrict__ feats,
+                                                                  int n, float* __restrict__ out, int* status) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    const int fp = P.fp, ka = max(fp, kHidden);
+    unsigned char* W1 = smem;
+    unsigned char* W2 = W1 + (size_t)kHidden * fp * 2;
+    unsigned char* W3 = W2 + (size_t)kHidden * kHidden * 2;
+    // two operand tiles: a tile's features (then its hidden layers), and the
+    // next tile's features arriving by cp.async meanwhile
+    unsigned char* Abuf[2] = {W3 + (size_t)tc::kN3 * kHidden * 2, W3 + (size_t)tc::kN3 * kHidden * 2 + (size_t)tc::kRows * ka * 2};
+    unsigned char* A = Abuf[0];
+    float* B1 = reinterpret_cast<float*>(Abuf[1] + (size_t)tc::kRows * ka * 2);
     float* B2 = B1 + kHidden;
     float* B3 = B2 + kHidden;
-    for (int t = threadIdx.x; t < kHidden * fp; t += blockDim.x) W1[(t / fp) * s1 + t % fp] = P.w1t[t];
-    for (int t = threadIdx.x; t < kHidden * kHidden; t += blockDim.x)
-        W2[(t / kHidden) * kW2Stride + t % kHidden] = P.w2t[t];
-    for (int t = threadIdx.x; t < 8 * kHidden; t += blockDim.x) W3[(t / kHidden) * kW2Stride + t % kHidden] = P.w3t[t];
-    for (int t = threadIdx.x; t < kHidden; t += blockDim.x) {
+    uint64_t* barp = reinterpret_cast<uint64_t*>(B3 + tc::kN3);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(barp + 1);
+    const int tid = threadIdx.x, warp = tid >> 5;
+
+    // weights in the canonical layout (rows of B are the layer's outputs);
+    // 4-byte loads: the packed weights are only 4-byte aligned
+    auto put_rows = [&](unsigned char* dst, const __nv_bfloat16* src, int rows, int valid_rows, int K) {
+        for (int t = tid; t < rows * (K / 8); t += tc::kThreads) {
+            const int r = t / (K / 8), kc = t % (K / 8);
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (r < valid_rows) {
+                const uint32_t* s = reinterpret_cast<const uint32_t*>(src + (size_t)r * K + kc * 8);
+                v = make_uint4(s[0], s[1], s[2], s[3]);
+            }
+            *reinterpret_cast<uint4*>(dst + tc::cm_offset(r, kc, rows)) = v;
+        }
+    };
+    put_rows(W1, P.w1t, kHidden, kHidden, fp);
+    put_rows(W2, P.w2t, kHidden, kHidden, kHidden);
+    put_rows(W3, P.w3t, tc::kN3, 8, kHidden);
+    for (int t = tid; t < kHidden; t += tc::kThreads) {
         B1[t] = P.b1[t];
         B2[t] = P.b2[t];
     }
-    if (threadIdx.x < 8) B3[threadIdx.x] = P.b3[threadIdx.x];
-    __syncthreads();
-
-    const int lane = threadIdx.x & 31, g = lane >> 2, t4 = lane & 3;
-    const int warp = blockIdx.x * kInferWarps + (threadIdx.x >> 5);
-    const int nwarps = gridDim.x * kInferWarps;
-    const int tiles = (n + 15) / 16;
-    for (int tile = warp; tile < tiles; tile += nwarps) {
-        const int r0 = tile * 16 + g, r1 = r0 + 8;
-        const bool v0 = r0 < n, v1 = r1 < n;
-        const unsigned* f0 = reinterpret_cast<const unsigned*>(feats + (size_t)(v0 ? r0 : 0) * fp);
-        const unsigned* f1 = reinterpret_cast<const unsigned*>(feats + (size_t)(v1 ? r1 : 0) * fp);
-        // layer 1
-        float acc[kHidden / 8][4];
-#pragma unroll
-        for (int j = 0; j < kHidden / 8; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
-        for (int kc = 0; kc < fp / 16; kc++) {
-            const int kw = kc * 8 + t4;  // 32-bit word index of columns 16kc + 2t4
-            const unsigned a0 = v0 ? __ldg(f0 + kw) : 0u, a1 = v1 ? __ldg(f1 + kw) : 0u;
-            const unsigned a2 = v0 ? __ldg(f0 + kw + 4) : 0u, a3 = v1 ? __ldg(f1 + kw + 4) : 0u;
-#pragma unroll
-            for (int j = 0; j < kHidden / 8; j++) {
-                const unsigned* wr = reinterpret_cast<const unsigned*>(W1 + (size_t)(8 * j + g) * s1 + 16 * kc);
-                mma_bf16(acc[j], a0, a1, a2, a3, wr[t4], wr[t4 + 4]);
-            }
-        }
-        unsigned A[kHidden / 16][4];
-#pragma unroll
-        for (int j = 0; j < kHidden / 8; j++) {
-            const float bx = B1[8 * j + 2 * t4], by = B1[8 * j + 2 * t4 + 1];
-            const unsigned lo = pack_bf16(fmaxf(acc[j][0] + bx, 0.f), fmaxf(acc[j][1] + by, 0.f));
-            const unsigned hi = pack_bf16(fmaxf(acc[j][2] + bx, 0.f), fmaxf(acc[j][3] + by, 0.f));
-            A[j >> 1][(j & 1) * 2 + 0] = lo;
-            A[j >> 1][(j & 1) * 2 + 1] = hi;
-        }
-        // layer 2
-#pragma unroll
-        for (int j = 0; j < kHidden / 8; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
-#pragma unroll
-        for (int kc = 0; kc < kHidden / 16; kc++) {
-#pragma unroll
-            for (int j = 0; j < kHidden / 8; j++) {
-                const unsigned* wr = reinterpret_cast<const unsigned*>(W2 + (size_t)(8 * j + g) * kW2Stride + 16 * kc);
-                mma_bf16(acc[j], A[kc][0], A[kc][1], A[kc][2], A[kc][3], wr[t4], wr[t4 + 4]);
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < kHidden / 8; j++) {
-            const float bx = B2[8 * j + 2 * t4], by = B2[8 * j + 2 * t4 + 1];
-            A[j >> 1][(j & 1) * 2 + 0] = pack_bf16(fmaxf(acc[j][0] + bx, 0.f), fmaxf(acc[j][1] + by, 0.f));
-            A[j >> 1][(j & 1) * 2 + 1] = pack_bf16(fmaxf(acc[j][2] + bx, 0.f), fmaxf(acc[j][3] + by, 0.f));
-        }
-        // layer 3 (outputs padded to 8)
-        float o[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-        for (int kc = 0; kc < kHidden / 16; kc++) {
-            const unsigned* wr = reinterpret_cast<const unsigned*>(W3 + (size_t)g * kW2Stride + 16 * kc);
-            mma_bf16(o, A[kc][0], A[kc][1], A[kc][2], A[kc][3], wr[t4], wr[t4 + 4]);
-        }
-        const int c0 = 2 * t4, c1 = 2 * t4 + 1;
-        if (v0 && c0 < P.dout) out[(size_t)r0 * P.dout + c0] = o[0] + B3[c0];
-        if (v0 && c1 < P.dout) out[(size_t)r0 * P.dout + c1] = o[1] + B3[c1];
-        if (v1 && c0 < P.dout) out[(size_t)r1 * P.dout + c0] = o[2] + B3[c0];
-        if (v1 && c1 < P.dout) out[(size_t)r1 * P.dout + c1] = o[3] + B3[c1];
+    if (tid < tc::kN3) B3[tid] = tid < 8 ? P.b3[tid] : 0.f;
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem);
+    const uint32_t sW1 = sbase, sW2 = sbase + (uint32_t)(W2 - smem), sW3 = sbase + (uint32_t)(W3 - smem);
+    uint32_t sA = sbase + (uint32_t)(A - smem);
+    const uint32_t bar = (uint32_t)__cvta_generic_to_shared(barp);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         (uint32_t)__cvta_generic_to_shared(slot)),
+                     "r"(tc::kCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = *slot;
+    const uint32_t lanes = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's TMEM lanes, column 0
+    const int row = tid;                                          // the tile row this thread's lane holds
+    uint32_t phase = 0;
+
+    // one layer: D (TMEM) = A (shared, 128 x K) x B (shared, N x K)^T
+    auto layer = [&](uint32_t b_addr, int K, int N) -> bool {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // A written by these threads
+        tc::fence_before();
+        __syncthreads();
+        tc::fence_after();
+        if (tid == 0) {
+            const uint32_t lbo_a = (tc::kRows / 8) * 128u, lbo_b = (uint32_t)(N / 8) * 128u;
+            const uint32_t id = tc::idesc_bf16(N);
+            for (int kk = 0; kk < K / 16; kk++) {
+                const uint64_t da = tc::smem_desc(sA + 2u * kk * lbo_a, lbo_a, 128u);
+                const uint64_t db = tc::smem_desc(b_addr + 2u * kk * lbo_b, lbo_b, 128u);
+                const uint32_t acc = kk > 0 ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(id), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                         : "memory");
+        }
+        const bool ok = tc::wait_phase(bar, phase);
+        if (!ok) (void)tc::wait_phase(bar, phase);  // let an MMA still in flight finish before TMEM is freed
+        phase ^= 1u;
+        tc::fence_after();
+        return __syncthreads_and(ok) != 0;
+    };
+    // hidden layer epilogue: bias, ReLU, BF16 into A as the next operand
+    auto hidden = [&](const float* bias) {
+        for (int c0 = 0; c0 < kHidden; c0 += 16) {
+            float v[16];
+            tc::tmem_ld16(lanes + (uint32_t)c0, v);
+            uint32_t p[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+                p[i] = pack_bf16(fmaxf(v[2 * i] + bias[c0 + 2 * i], 0.f), fmaxf(v[2 * i + 1] + bias[c0 + 2 * i + 1], 0.f));
+            *reinterpret_cast<uint4*>(A + tc::cm_offset(row, c0 / 8, tc::kRows)) = make_uint4(p[0], p[1], p[2], p[3]);
+            *reinterpret_cast<uint4*>(A + tc::cm_offset(row, c0 / 8 + 1, tc::kRows)) = make_uint4(p[4], p[5], p[6], p[7]);
+        }
+    };
+
+    const bool al16 = ((uintptr_t)feats & 15) == 0;
+    const int tiles = (n + tc::kRows - 1) / tc::kRows;
+    // a tile's features into buf by 16-byte cp.async (rows past n zero-filled)
+    auto prefetch = [&](int tile, unsigned char* buf) {
+        const int r0 = tile * tc::kRows;
+        for (int t = tid; t < tc::kRows * (fp / 8); t += tc::kThreads) {
+            const int r = t / (fp / 8), kc = t % (fp / 8);
+            const bool in = r0 + r < n;
+            const __nv_bfloat16* src = feats + (in ? (size_t)(r0 + r) * fp + kc * 8 : 0);
+            const uint32_t dst = (uint32_t)__cvta_generic_to_shared(buf + tc::cm_offset(r, kc, tc::kRows));
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(in ? 16 : 0)
+                         : "memory");
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    if (al16 && blockIdx.x < tiles) prefetch(blockIdx.x, Abuf[0]);
+    int cur = 0;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, cur ^= 1) {
+        const int r0 = tile * tc::kRows;
+        A = Abuf[cur];
+        sA = sbase + (uint32_t)(A - smem);
+        if (al16) {
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            // the other buffer's last reader (the previous tile's layer 3)
+            // completed before this tile began
+            if (tile + (int)gridDim.x < tiles) prefetch(tile + gridDim.x, Abuf[cur ^ 1]);
+        }
+        for (int t = tid; !al16 && t < tc::kRows * (fp / 8); t += tc::kThreads) {
+            const int r = t / (fp / 8), kc = t % (fp / 8);
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (r0 + r < n) {
+                // feature rows not 16-byte aligned: 2-byte loads, synchronously
+                const unsigned short* h = reinterpret_cast<const unsigned short*>(feats + (size_t)(r0 + r) * fp + kc * 8);
+                v = make_uint4(h[0] | ((uint32_t)h[1] << 16), h[2] | ((uint32_t)h[3] << 16),
+                               h[4] | ((uint32_t)h[5] << 16), h[6] | ((uint32_t)h[7] << 16));
+            }
+            *reinterpret_cast<uint4*>(A + tc::cm_offset(r, kc, tc::kRows)) = v;
+        }
+        bool ok = layer(sW1, fp, kHidden);
+        if (ok) {
+            hidden(B1);
+            ok = layer(sW2, kHidden, kHidden);
+        }
+        if (ok) {
+            hidden(B2);
+            ok = layer(sW3, kHidden, tc::kN3);
+        }
+        float v[16];
+        if (ok) tc::tmem_ld16(lanes, v);
+        if (r0 + row < n)
+            for (int c = 0; c < P.dout; c++) out[(size_t)(r0 + row) * P.dout + c] = ok ? v[c] + B3[c] : __int_as_float(0x7fc00000);
+        if (!ok) {
+            if (tid == 0) atomicExch(status, 1);
+            break;
+        }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");  // a prefetch left by a failed tile
+    tc::fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tc::kCols));
 }
 
 // fp32 [in][out] (row-major, as trained) -> bf16 [out_pad][in_pad], zero padded
@@ -312,8 +451,11 @@ __global__ void k_apply(FGrid G, float* X, size_t ns, int n, const float* __rest
         }
         if (total < min_count) continue;
         for (int l = 0; l < d; l++) {
+            // a NaN displacement (inference that did not complete) leaves the point in place
+            const float dl = delta[(size_t)p * d + l];
+            if (dl != dl) continue;
             float* x = X + (size_t)l * ns + p;
-            *x = fminf(fmaxf(__fmaf_rn(eps, delta[(size_t)p * d + l], *x), 0.f), 1.f);
+            *x = fminf(fmaxf(__fmaf_rn(eps, dl, *x), 0.f), 1.f);
         }
     }
 }
@@ -574,7 +716,8 @@ void infer(const egg_mlp& m, const __nv_bfloat16* feats, int n, float* out, Buff
     // weights: fp32 on the device, then packed bf16
     Params P{F, kHidden, m.d, nullptr};
     const size_t pcount = P.count();
-    const size_t wbytes = 4 * pcount + 2 * ((size_t)kHidden * fp + (size_t)kHidden * kHidden + 8 * kHidden) + 4 * 8;
+    const size_t wbytes =
+        4 * pcount + 2 * ((size_t)kHidden * fp + (size_t)kHidden * kHidden + 8 * kHidden) + 4 * 8 + 16;
     if (wbytes > B.w_cap) {
         if (B.w) EGG_CHECK(cudaFree(B.w));
         B.w = nullptr;
@@ -598,11 +741,24 @@ void infer(const egg_mlp& m, const __nv_bfloat16* feats, int n, float* out, Buff
     k_pack_t<<<grid_for(8 * kHidden), 256, 0, st>>>(P.w3(), kHidden, m.d, K.w3t, kHidden, 8);
     EGG_CHECK(cudaMemsetAsync(K.b3, 0, 4 * 8, st));
     EGG_CHECK(cudaMemcpyAsync(K.b3, P.b3(), 4 * m.d, cudaMemcpyDeviceToDevice, st));
-    const size_t smem = infer_smem(fp);
-    EGG_CHECK(cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int tiles = (n + 15) / 16;
-    const int blocks = std::max(1, std::min((tiles + kInferWarps - 1) / kInferWarps, 148 * 2));
-    k_mlp_infer<<<blocks, 32 * kInferWarps, smem, st>>>(K, feats, n, out);
+    int* status = reinterpret_cast<int*>(K.b3 + 8);
+    EGG_CHECK(cudaMemsetAsync(status, 0, sizeof(int), st));
+    const size_t smem = tc::smem_bytes(fp);
+    EGG_CHECK(cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int tiles = (n + tc::kRows - 1) / tc::kRows;
+    const int blocks = std::max(1, std::min(tiles, 148));
+    k_mlp_infer_tc<<<blocks, tc::kThreads, smem, st>>>(K, feats, n, out, status);
+}
+
+// the status word of the last inference (1: an MMA never completed)
+int infer_status(Buffers& B, const egg_mlp& m, cudaStream_t st) {
+    const int fp = feat_pad(m.d), F = feat_dim(m.d);
+    const size_t pcount = Params{F, kHidden, m.d, nullptr}.count();
+    const char* base = (const char*)B.w + 4 * pcount + 2 * ((size_t)kHidden * fp + (size_t)kHidden * kHidden + 8 * kHidden) + 4 * 8;
+    int v = 0;
+    EGG_CHECK(cudaMemcpyAsync(&v, base, sizeof(int), cudaMemcpyDeviceToHost, st));
+    EGG_CHECK(cudaStreamSynchronize(st));
+    return v;
 }
 
 
@@ -681,6 +837,8 @@ int api_forward(const egg_mlp* m, const float* feats, int64_t n, float* out) {
     if (!dev_out) EGG_CHECK(cudaMemcpyAsync(out, od, 4 * (size_t)n * m->d, cudaMemcpyDeviceToHost, st));
     EGG_CHECK(cudaStreamSynchronize(st));
     EGG_CHECK(cudaGetLastError());
+    if (infer_status(g_buf, *m, st) != 0)
+        throw ArgError{EGG_ERR_INTERNAL, "tensor-core inference did not complete (mbarrier wait limit)"};
     return EGG_OK;
 }
 
