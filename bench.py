@@ -80,6 +80,9 @@ def parse():
     ap.add_argument("--sync-iterations", action="store_true",
                     help="count the reference CPU SynC's iterations on the workload (brute-force GPU SynC)")
     ap.add_argument("--sync-max-iter", type=int, default=300)
+    ap.add_argument("--profile-warm", action="store_true",
+                    help="for ncu: one warm-up run and one warm-started run of the workload (learned "
+                         "warm start), no timing")
     ap.add_argument("--stage-split", action="store_true",
                     help="per-phase split of the loop graph's time (iterations 0-11, 12-59, 60+) from the "
                          "per-iteration %%globaltimer stamps, and the slowest iterations")
@@ -104,6 +107,25 @@ def profile_run(args):
     torch.cuda.synchronize(dev)
     print(json.dumps({"profile_run": True, "n": len(c["X"]), "iterations": info["iterations"],
                       "launches_per_run": info["launches"]}))
+
+
+def profile_warm(args):
+    """One warm-up run and one run with the learned warm start (features,
+    tensor-core inference, displacement, then the plain loop)."""
+    import torch
+
+    from eggsync import data, egg_sync, warm
+
+    dev = torch.device("cuda", 0)
+    c = data.c5(args.seed, n=args.n)
+    Xd = torch.from_numpy(c["X"]).to(dev)
+    lab = torch.empty(len(c["X"]), dtype=torch.int32, device=dev)
+    model = warm.default_model(3)
+    for k in range(2):
+        _, info = egg_sync(Xd, c["eps"], labels_out=lab, warm_start=model)
+    torch.cuda.synchronize(dev)
+    print(json.dumps({"profile_warm": True, "n": len(c["X"]), "iterations": info["iterations"],
+                      "warm_ms": info["warm_ms"]}))
 
 
 def stage_split(args):
@@ -725,6 +747,9 @@ def main():
         return
     if args.stage_split:
         stage_split(args)
+        return
+    if args.profile_warm:
+        profile_warm(args)
         return
     if args.sync_iterations:
         sync_iterations(args)
