@@ -54,6 +54,21 @@ def test_forward_bf16_tensor_cores_match_oracle():
     assert np.array_equal(y7, y[:37])
 
 
+@pytest.mark.parametrize("d", [1, 2])
+def test_forward_lower_dims_match_oracle(d):
+    """The tensor-core network for d = 1 and 2 (narrower feature rows than
+    d = 3), on 1,000 points: seven full 128-point tiles and a partial one."""
+    rng = np.random.default_rng(10 + d)
+    X = data.min_max_normalize(rng.standard_normal((1000, d)) * 0.1 + 0.5)
+    f = warm.features(X, 0.03)
+    m = random_model(d, seed=d)
+    y = warm.forward(m, f)
+    ref = M.forward(m.w, f, d, emulate_bf16=True)
+    assert y.shape == ref.shape == (len(X), d)
+    assert np.abs(y - ref).max() <= 1e-2 * np.abs(ref).max()
+    assert np.array_equal(warm.forward(m, f[:129]), y[:129])
+
+
 def test_gradient_matches_oracle():
     c = small3d(4000)
     f = warm.features(c["X"], c["eps"])[:256]
