@@ -296,17 +296,26 @@ def grid_bytes(n, d, width, cells, n_outer):
     """Algorithmic bytes of one full grid build from device-resident points
     (egg_sync_grid, the grid of EGG_SynC.cu:248-341): the input transpose
     (row-major read, per-dimension write, original index), the grid check's
-    copy, per radix pass the digit reads through the permutation (all d
-    coordinates in the first, sub-cell pass; one per later pass) and the
-    permutation read/write, the tile histograms, the gather into sorted
-    order, the cell heads and records, the outer ranges."""
-    digits = 1 if width <= 256 else 2
-    passes = 1 + d * digits
-    tiles = (n + 4095) // 4096
+    copy, the radix sort, the tile histograms, the gather into sorted
+    order, the cell heads and records, the outer ranges.  The sort: for
+    d <= 3 with at most 256 cells per dimension one 32-bit key per point is
+    computed once (d coordinates read, key and position written) and 1 + d
+    passes each read the keys for the histogram and move (key, position)
+    pairs (the last pass writes positions only); otherwise each pass reads
+    its digit through the permutation (all d coordinates in the first,
+    sub-cell pass) and reads and writes the permutation."""
+    tiles = (n + 2047) // 2048                # 2048-point tiles
     per_point = (4 * d + 4 * d + 4)          # transpose
     per_point += 8 * d                       # grid check: read Xn, write X
-    per_point += 4 * d + 4 * d + 4           # sub-cell pass: hist + scatter (first pass reads no permutation)
-    per_point += (passes - 1) * (8 + 12)     # later passes: hist (perm + digit), scatter (perm + digit + perm out)
+    if d <= 3 and width <= 256:
+        passes = 1 + d
+        per_point += 4 * d + 8               # keys: coordinates in; key, position out
+        per_point += passes * (4 + 16) - 4   # per pass: hist (key), scatter (key, position in and out)
+    else:
+        digits = 1 if width <= 256 else 2
+        passes = 1 + d * digits
+        per_point += 4 * d + 4 * d + 4       # sub-cell pass: hist + scatter (first pass reads no permutation)
+        per_point += (passes - 1) * (8 + 12)  # later passes: hist (perm + digit), scatter (perm + digit + perm out)
     per_point += 4 + 4 * d + 4 + 4 * d + 4   # gather: perm, Xn, orig in; X, orig_tmp out
     per_point += 4 * d + 4 + 4 + 4           # heads: X, orig_tmp in; cell_of, orig out
     hist = passes * tiles * 256 * 4 * 4      # histogram write, scan read + write, scatter read

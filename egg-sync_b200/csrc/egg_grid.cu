@@ -433,6 +433,9 @@ __device__ __forceinline__ void heads_finalize_body(const Geom& g, const Work& w
     EGG_SKIP_IF_UNCHANGED(w.ctrl);
     const int d = D > 0 ? D : g.d;
     const int i = bx * blockDim.x + threadIdx.x;
+    // the outer-ranges kernel that follows ORs the column masks in
+    // (n_outer = width^od <= n: one thread per point covers every column)
+    if (g.od < d && w.colmask != nullptr && i < g.n_outer) w.colmask[i] = 0ull;
     int head = 0;
     if (i < g.n) {
         head = (i == 0);
@@ -470,13 +473,23 @@ __device__ __forceinline__ void outer_ranges_body(const Geom& g, const Work& w, 
     const int M = w.ctrl[kCtrlM];
     const bool cols = g.od < g.d && w.colmask != nullptr;
     const int* z = w.cell_dims + (size_t)g.od * g.ns;
-    for (int o = bx * blockDim.x + threadIdx.x; o <= g.n_outer; o += gx * blockDim.x) {
-        const int b = lower_bound_i(w.cell_outer, 0, M, o);
-        w.outer_begin[o] = b;
-        if (cols && o < g.n_outer) {
-            unsigned long long m = 0;
-            for (int c = b; c < M && w.cell_outer[c] == o; c++) m |= 1ull << (z[c] / g.zblk);
-            w.colmask[o] = m;
+    // A thread per cell: cell c is the first cell of every column o with
+    // cell_outer[c - 1] < o <= cell_outer[c] (columns in between are empty;
+    // c = M closes the last one), so outer_begin[o] is the first cell of a
+    // column at or after o, each entry written once.  A column's mask of
+    // occupied blocks of dimension od is the OR over its cells: one atomic
+    // per column and warp (the heads kernel zeroed the masks).
+    for (int c = bx * blockDim.x + threadIdx.x; c <= M; c += gx * blockDim.x) {
+        const int oc = c < M ? w.cell_outer[c] : g.n_outer;
+        const int op = c > 0 ? w.cell_outer[c - 1] : -1;
+        for (int o = op + 1; o <= oc; o++) w.outer_begin[o] = c;
+        if (cols && c < M) {
+            const unsigned long long bit = 1ull << (z[c] / g.zblk);
+            const unsigned peers = __match_any_sync(__activemask(), oc);
+            const unsigned lo = __reduce_or_sync(peers, (unsigned)bit);
+            const unsigned hi = __reduce_or_sync(peers, (unsigned)(bit >> 32));
+            if ((threadIdx.x & 31) == __ffs(peers) - 1)
+                atomicOr(w.colmask + oc, ((unsigned long long)hi << 32) | lo);
         }
     }
 }
