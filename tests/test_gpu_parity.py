@@ -2,8 +2,8 @@
 and against the reference EGG-SynC's own results (fixtures).
 
 Bars: grid, counts, flags and labels are bit-exact (integer work); positions
-within 1e-5 absolute of the FP64 oracle per iteration (the tolerance the
-north-star spec states for [0,1]-normalised data)."""
+within 1e-5 absolute of the FP64 oracle per iteration (coordinates are
+min-max normalised to [0, 1])."""
 import numpy as np
 import pytest
 
